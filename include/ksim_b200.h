@@ -1,0 +1,201 @@
+/*
+ * ksim_b200.h — C ABI of the B200-native ksim sampler.
+ *
+ * This is the drop-in boundary for ksim's sampling hot path
+ * (FlatProgram -> samples).  Every entry point takes plain pointers and sizes;
+ * no C++, Python or torch type crosses it.  Device work runs in hand-written
+ * sm_100a CUDA kernels inside libksim_b200.so.
+ *
+ * Reference interfaces replaced (paths inside the ksim project):
+ *   kokkos_sim.Component(graphs, num_f)        src/cpp/ksim/kokkos_sim.cpp:67-152
+ *   Component.sample(f_sel, seed)              src/cpp/ksim/kokkos_sim.cpp:188-241
+ *   Component.eval_abs(graph, params)          src/cpp/ksim/kokkos_sim.cpp:157-185
+ *   Component.n_out                            src/cpp/ksim/kokkos_sim.cpp:250-251
+ *   KokkosProgramSampler.sample(f, seed)       src/python/ksim/sample/sampler.py:57-67
+ *   per-graph dict layout (_graph_to_dict)     src/python/ksim/sample/sampler.py:21-43
+ *
+ * Errors are status codes; the message of the last failing call on the
+ * calling thread is available from ksim_last_error().  KSIM_ERR_INVALID_ARGUMENT
+ * is what the reference reports as std::invalid_argument (Python ValueError).
+ */
+#ifndef KSIM_B200_H
+#define KSIM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KSIM_B200_ABI_VERSION 1
+
+typedef enum ksim_status {
+    KSIM_OK = 0,
+    KSIM_ERR_INVALID_ARGUMENT = 1, /* bad shape / count / pointer (ValueError) */
+    KSIM_ERR_MALFORMED_PROGRAM = 2, /* a graph's arrays are inconsistent        */
+    KSIM_ERR_CUDA = 3,              /* a CUDA runtime call failed               */
+    KSIM_ERR_OUT_OF_MEMORY = 4,     /* device or pinned host allocation failed  */
+    KSIM_ERR_TIMEOUT = 5,           /* a bounded device wait ran out            */
+    KSIM_ERR_UNSUPPORTED = 6,       /* size beyond what this build handles      */
+    KSIM_ERR_NOT_FOUND = 7,         /* unknown request / handle                 */
+    KSIM_ERR_CANCELLED = 8,         /* request cancelled before completion      */
+    KSIM_ERR_NO_DEVICE = 9,         /* no CUDA device visible                   */
+    KSIM_ERR_INTERNAL = 10
+} ksim_status;
+
+/* Uniform streams for the per-output Bernoulli draw.
+ *   KSIM_RNG_XORSHIFT: the reference's per-shot stream, bit-identical to
+ *     kokkos_sim for the same seed (seed mixing kokkos_sim.cpp:215-217,
+ *     xorshift64 13/7/17 kokkos_sim.cpp:43-46).
+ *   KSIM_RNG_PHILOX: counter-based Philox4x32-10 (Salmon et al., SC'11),
+ *     key = (seed lo32, seed hi32), counter = (shot lo32, shot hi32, output, 0),
+ *     u = ((x1:x0) >> 11) * 2^-53.  Any shot range can be recomputed alone. */
+enum { KSIM_RNG_XORSHIFT = 0, KSIM_RNG_PHILOX = 1 };
+
+/* Advisory status bits raised by the kernels (results are never changed). */
+enum {
+    KSIM_FLAG_INT64_RISK = 1u,      /* a Z[w] coefficient exceeded 2^62 before a multiply */
+    KSIM_FLAG_PREV_NONPOSITIVE = 2u,/* a marginal |A| was <= 0 at a Bernoulli step       */
+    KSIM_FLAG_NAN = 4u,             /* p1/prev was NaN                                   */
+    KSIM_FLAG_WAIT_TIMEOUT = 8u     /* a bounded device wait gave up                     */
+};
+
+/* One FlatScalarGraph, exactly the 19 arrays of the reference's per-graph dict
+ * (sampler.py:21-43), C-contiguous, borrowed for the duration of the call.
+ * G = pf_phase_idx.shape[0], P = np_params.shape[2], T* = family widths
+ * (kokkos_sim.cpp:98-103).  Arrays of a zero-sized shape may be NULL. */
+typedef struct ksim_graph_desc {
+    int32_t G, P, Tnp, Thp, Tpp, Tph;
+    const uint8_t *np_phases;   /* (G,Tnp)   */
+    const uint8_t *np_params;   /* (G,Tnp,P) */
+    const int32_t *np_counts;   /* (G,)      */
+    const uint8_t *hp_coeffs;   /* (G,Thp)   */
+    const uint8_t *hp_params;   /* (G,Thp,P) */
+    const uint8_t *pp_psi_c;    /* (G,Tpp)   */
+    const uint8_t *pp_psi_p;    /* (G,Tpp,P) */
+    const uint8_t *pp_phi_c;    /* (G,Tpp)   */
+    const uint8_t *pp_phi_p;    /* (G,Tpp,P) */
+    const uint8_t *ph_alpha;    /* (G,Tph)   */
+    const uint8_t *ph_alpha_p;  /* (G,Tph,P) */
+    const uint8_t *ph_beta;     /* (G,Tph)   */
+    const uint8_t *ph_beta_p;   /* (G,Tph,P) */
+    const int32_t *ph_counts;   /* (G,)      */
+    const uint8_t *pf_phase_idx;   /* (G,)   */
+    const int32_t *pf_floatfactor; /* (G,4)  */
+    const int32_t *pf_power2;      /* (G,)   */
+    const float *pf_approx_f32;    /* (G,2) complex64 as float pairs */
+    int32_t pf_has_approx;
+} ksim_graph_desc;
+
+typedef struct ksim_component ksim_component;
+typedef struct ksim_program ksim_program;
+
+/* ---- library ---------------------------------------------------------- */
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *ksim_last_error(void);
+int32_t ksim_abi_version(void);
+/* Number of visible CUDA devices (0 when none; never fails). */
+int32_t ksim_device_count(void);
+
+/* ---- component: kokkos_sim.Component ----------------------------------- */
+
+/* Validate, pack into the device structure-of-arrays image and upload.
+ * Replaces KokkosTsimComponent(graphs, F), kokkos_sim.cpp:67-152.
+ * device < 0 selects the calling thread's current device. */
+ksim_status ksim_component_create(const ksim_graph_desc *graphs, int32_t n_graphs,
+                                  int32_t num_f, int32_t device,
+                                  ksim_component **out);
+void ksim_component_destroy(ksim_component *c);
+int32_t ksim_component_n_out(const ksim_component *c);   /* n_graphs - 1 */
+int32_t ksim_component_num_f(const ksim_component *c);
+int32_t ksim_component_n_graphs(const ksim_component *c);
+int32_t ksim_component_words(const ksim_component *c);   /* 64-bit words per parameter vector */
+int64_t ksim_component_image_bytes(const ksim_component *c);
+
+/* Host buffers, synchronous.  f_sel: (B, num_f) uint8 C-contiguous; out:
+ * (B, max(n_out,1)) uint8.  Replaces Component.sample, kokkos_sim.cpp:188-241
+ * (bit-identical to it with rng_mode = KSIM_RNG_XORSHIFT). */
+ksim_status ksim_component_sample(ksim_component *c, const uint8_t *f_sel, int64_t B,
+                                  uint64_t seed, int32_t rng_mode, uint8_t *out);
+
+/* Device buffers, asynchronous on `stream` (a cudaStream_t; NULL = legacy
+ * default stream).  Shot s of this call uses shot index shot_offset + s for
+ * its uniforms, so a shot range split across calls or GPUs reproduces the
+ * single-call result.  out_stride = bytes between output rows (>= n_out);
+ * out_col0 = first column written.  amp (nullable): (B, n_out+1) float64 of
+ * |A_k| per graph, for parity checks. */
+ksim_status ksim_component_sample_device(ksim_component *c, const uint8_t *d_f_sel,
+                                         int64_t B, int64_t shot_offset, uint64_t seed,
+                                         int32_t rng_mode, uint8_t *d_out,
+                                         int64_t out_stride, int64_t out_col0,
+                                         double *d_amp, void *stream);
+
+/* |amplitude| of graph `graph` for B explicit parameter rows (B, P) uint8.
+ * Replaces Component.eval_abs, kokkos_sim.cpp:157-185.  Host buffers. */
+ksim_status ksim_component_eval_abs(ksim_component *c, int32_t graph, const uint8_t *params,
+                                    int64_t B, int64_t P, double *out);
+/* Complex amplitude (B, 2) float64 (re, im) of the same evaluation. */
+ksim_status ksim_component_eval(ksim_component *c, int32_t graph, const uint8_t *params,
+                                int64_t B, int64_t P, double *out_re_im);
+/* Per-term exact Z[w] numerators: out (B, G, 5) int64 = (a, b, c, d, pw) in
+ * the basis (1, w, i, conj w) after the term's last renormalisation step
+ * (zx_eval.hpp:101-165 schedule), before the prefactor power2. */
+ksim_status ksim_component_eval_terms(ksim_component *c, int32_t graph, const uint8_t *params,
+                                      int64_t B, int64_t P, int64_t *out);
+
+/* OR of KSIM_FLAG_* raised by this component's kernels since the last reset. */
+ksim_status ksim_component_status(ksim_component *c, uint32_t *flags, int32_t reset);
+
+/* Launch shape of the plain sampler for this component: threads per CTA
+ * (a multiple of 32, <= 256), whether term chunks are staged in shared memory
+ * by TMA bulk copies, and the staging slot size in bytes (>= the largest term
+ * record, a multiple of 16).  Zero / negative values keep the current value. */
+ksim_status ksim_component_set_launch(ksim_component *c, int32_t threads, int32_t staged,
+                                      int32_t slot_bytes);
+ksim_status ksim_component_get_launch(const ksim_component *c, int32_t *threads, int32_t *staged,
+                                      int32_t *slot_bytes);
+/* Image statistics: terms, terms on the exact (overflow-risk) path, columns,
+ * largest term record in bytes. */
+ksim_status ksim_component_stats(const ksim_component *c, int64_t *n_terms, int64_t *n_slow_terms,
+                                 int64_t *n_columns, int64_t *max_term_bytes);
+
+/* ---- program: KokkosProgramSampler ------------------------------------- */
+
+/* A FlatProgram: components (borrowed, must outlive the program, all on one
+ * device), each with its f_selection (columns of the full f matrix), and
+ * output_order (distinct values, one per output of the concatenated
+ * components).  Replaces KokkosProgramSampler.__init__, sampler.py:48-55. */
+ksim_status ksim_program_create(ksim_component *const *comps, int32_t n_comps,
+                                const int32_t *const *f_selection, const int32_t *f_sel_len,
+                                const int32_t *output_order, int32_t n_outputs,
+                                ksim_program **out);
+void ksim_program_destroy(ksim_program *p);
+int32_t ksim_program_n_outputs(const ksim_program *p);
+/* Smallest row width an f matrix must have (max f_selection + 1). */
+int32_t ksim_program_min_f_cols(const ksim_program *p);
+
+/* f_params: (B, n_f_cols) uint8 host; out: (B, n_outputs) uint8 host.
+ * Component k is seeded with seed + 0x9E37*k and the outputs are permuted by
+ * argsort(output_order), as sampler.py:57-67 does; the f_selection gather and
+ * the permutation run on the device. */
+ksim_status ksim_program_sample(ksim_program *p, const uint8_t *f_params, int64_t B,
+                                int64_t n_f_cols, uint64_t seed, int32_t rng_mode, uint8_t *out);
+/* Same on device buffers, asynchronous on `stream`. */
+ksim_status ksim_program_sample_device(ksim_program *p, const uint8_t *d_f_params, int64_t B,
+                                       int64_t n_f_cols, int64_t shot_offset, uint64_t seed,
+                                       int32_t rng_mode, uint8_t *d_out, void *stream);
+
+/* ---- measurement --------------------------------------------------------- */
+
+/* Integer-pipe throughput of this GPU for the sampler's instruction mix
+ * (32-bit add / shift / logic), in int32 lane-operations per second: the
+ * roofline denominator of the sampling kernels.  No reference counterpart. */
+ksim_status ksim_measure_int_peak(int32_t device, double *ops_per_s, double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KSIM_B200_H */

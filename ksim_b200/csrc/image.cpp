@@ -1,0 +1,392 @@
+// image.cpp — validation and packing of a component into the device image.
+//
+// Input: the reference's per-graph arrays (sampler.py:21-43 dict layout,
+// kokkos_sim.cpp:91-129 field set).  Output: one byte image
+//   [GraphDir x n_graphs][term stream of graph 0][term stream of graph 1]...
+// Each term record (16-byte aligned):
+//   u32 n_np | n_hp<<16, u32 n_pp | n_ph<<16, u32 pf_idx | nu_np<<8 | flags<<16,
+//   i32 power2, i32 floatfactor[4], [f64 approx re, im], then the columns.
+// Column records hold the parameter masks as W 64-bit words (bit j = param j)
+// and one constant word:
+//   NodePhases  [mask W][phase | reduce<<3]               (count = np_counts[g])
+//   HalfPi      [mask W][coeff & 7]                       (zero coeffs dropped)
+//   PiProducts  [psi W][phi W][psi_c | phi_c<<1]          (identically-zero dropped)
+//   PhasePairs  [alpha W][beta W][a | b<<3 | nu table<<8] (count = ph_counts[g])
+// Dropped columns contribute nothing in the reference either (a zero HalfPi
+// coefficient adds 0 to the phase sum; a PiProducts column whose psi or phi is
+// identically 0 adds psi*phi = 0).
+#include "image.h"
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+
+#include "zring.cuh"
+
+namespace ksim {
+
+namespace {
+
+constexpr int kWords[] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 16};
+
+void put32(std::vector<uint8_t> &b, uint32_t v)
+{
+    uint8_t t[4];
+    std::memcpy(t, &v, 4);
+    b.insert(b.end(), t, t + 4);
+}
+void put64(std::vector<uint8_t> &b, uint64_t v)
+{
+    uint8_t t[8];
+    std::memcpy(t, &v, 8);
+    b.insert(b.end(), t, t + 8);
+}
+
+// sigma_k(z) for the embedding w -> e^{i k pi/4}.
+std::complex<double> embed(const int64_t z[4], int k)
+{
+    const double th = k * M_PI / 4;
+    const std::complex<double> w(std::cos(th), std::sin(th));
+    return (double)z[0] + (double)z[1] * w + (double)z[2] * (w * w) + (double)z[3] * std::conj(w);
+}
+
+double max_embed(const int64_t z[4])
+{
+    double m = 0;
+    for (int k = 1; k < 8; k += 2) m = std::max(m, std::abs(embed(z, k)));
+    return m;
+}
+
+void unit(int k, int64_t out[4])
+{
+    static const int64_t t[8][4] = {{1, 0, 0, 0}, {0, 1, 0, 0}, {0, 0, 1, 0}, {0, 0, 0, -1},
+                                    {-1, 0, 0, 0}, {0, -1, 0, 0}, {0, 0, -1, 0}, {0, 0, 0, 1}};
+    for (int i = 0; i < 4; ++i) out[i] = t[k & 7][i];
+}
+
+// 1 + w^a + w^b - w^(a+b)
+void phase_pair(int a, int b, int64_t out[4])
+{
+    int64_t u[4], v[4], x[4];
+    unit(a, u); unit(b, v); unit(a + b, x);
+    for (int i = 0; i < 4; ++i) out[i] = u[i] + v[i] - x[i];
+    out[0] += 1;
+}
+
+struct Bits {
+    const uint8_t *row;  // P bytes
+};
+
+// Pack one P-byte mask row into W words; false if a byte is neither 0 nor 1.
+bool pack_mask(const uint8_t *row, int P, int W, uint64_t *out)
+{
+    for (int w = 0; w < W; ++w) out[w] = 0;
+    for (int j = 0; j < P; ++j) {
+        const uint8_t b = row[j];
+        if (b > 1) return false;
+        out[j >> 6] |= (uint64_t)b << (j & 63);
+    }
+    return true;
+}
+
+bool all_zero(const uint64_t *m, int W)
+{
+    for (int w = 0; w < W; ++w)
+        if (m[w]) return false;
+    return true;
+}
+
+}  // namespace
+
+int supported_words(int needed)
+{
+    for (int w : kWords)
+        if (w >= needed) return w;
+    return -1;
+}
+
+uint32_t zw_valuation(const int64_t z[4])
+{
+    if (!z[0] && !z[1] && !z[2] && !z[3]) return NU_ZERO;
+    // z * conj(z) = p + q sqrt2, conj(a,b,c,d) = (a,d,-c,b); N(z) = p^2 - 2 q^2
+    typedef __int128 i128;
+    const i128 a = z[0], b = z[1], c = z[2], d = z[3];
+    const i128 ca = a, cb = d, cc = -c, cd = b;
+    const i128 p = a * ca + b * cd - c * cc + d * cb;
+    const i128 q = a * cb + b * ca + c * cd + d * cc;
+    i128 n = p * p - 2 * q * q;
+    if (n < 0) n = -n;
+    uint32_t v = 0;
+    while (n != 0 && (n & 1) == 0) {
+        n >>= 1;
+        ++v;
+    }
+    return v;
+}
+
+int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, std::string &err)
+{
+    if (n_graphs < 1) {
+        err = "a component needs at least one graph (the normalisation graph)";
+        return KSIM_ERR_INVALID_ARGUMENT;
+    }
+    if (F < 0) {
+        err = "num_f must be >= 0";
+        return KSIM_ERR_INVALID_ARGUMENT;
+    }
+    if (!gs) {
+        err = "graphs is NULL";
+        return KSIM_ERR_INVALID_ARGUMENT;
+    }
+    const int n_out = n_graphs - 1;
+    int64_t need_bits = (int64_t)F + n_out;
+    for (int k = 0; k < n_graphs; ++k) {
+        const ksim_graph_desc &g = gs[k];
+        if (g.G < 0 || g.P < 0 || g.Tnp < 0 || g.Thp < 0 || g.Tpp < 0 || g.Tph < 0) {
+            err = "graph " + std::to_string(k) + ": negative dimension";
+            return KSIM_ERR_MALFORMED_PROGRAM;
+        }
+        need_bits = std::max<int64_t>(need_bits, g.P);
+    }
+    const int W = supported_words((int)std::max<int64_t>(1, (need_bits + 63) / 64));
+    if (W < 0 || need_bits > 64 * 16) {
+        err = "parameter vector of " + std::to_string(need_bits) +
+              " bits exceeds the 1024 this build supports";
+        return KSIM_ERR_UNSUPPORTED;
+    }
+    const int R1 = rec1_words(W), R2 = rec2_words(W);
+
+    img = HostImage();
+    img.n_graphs = n_graphs;
+    img.F = F;
+    img.n_out = n_out;
+    img.W = W;
+    img.gdir.resize(n_graphs);
+    img.term_off.resize(n_graphs);
+    std::vector<uint8_t> &out = img.bytes;
+    out.resize(sizeof(GraphDir) * (size_t)n_graphs, 0);
+
+    std::vector<uint64_t> mask(2 * W);
+    std::vector<uint8_t> zero_row;
+
+    for (int k = 0; k < n_graphs; ++k) {
+        const ksim_graph_desc &g = gs[k];
+        const int G = g.G, P = g.P;
+        const std::string gname = "graph " + std::to_string(k);
+        auto need = [&](const void *p, int64_t n, const char *name) -> bool {
+            if (n > 0 && !p) {
+                err = gname + ": " + name + " is NULL but has " + std::to_string(n) + " elements";
+                return false;
+            }
+            return true;
+        };
+        if (!need(g.np_phases, (int64_t)G * g.Tnp, "np_phases") ||
+            !need(g.np_params, (int64_t)G * g.Tnp * P, "np_params") ||
+            !need(g.np_counts, G, "np_counts") || !need(g.hp_coeffs, (int64_t)G * g.Thp, "hp_coeffs") ||
+            !need(g.hp_params, (int64_t)G * g.Thp * P, "hp_params") ||
+            !need(g.pp_psi_c, (int64_t)G * g.Tpp, "pp_psi_c") ||
+            !need(g.pp_psi_p, (int64_t)G * g.Tpp * P, "pp_psi_p") ||
+            !need(g.pp_phi_c, (int64_t)G * g.Tpp, "pp_phi_c") ||
+            !need(g.pp_phi_p, (int64_t)G * g.Tpp * P, "pp_phi_p") ||
+            !need(g.ph_alpha, (int64_t)G * g.Tph, "ph_alpha") ||
+            !need(g.ph_alpha_p, (int64_t)G * g.Tph * P, "ph_alpha_p") ||
+            !need(g.ph_beta, (int64_t)G * g.Tph, "ph_beta") ||
+            !need(g.ph_beta_p, (int64_t)G * g.Tph * P, "ph_beta_p") ||
+            !need(g.ph_counts, G, "ph_counts") || !need(g.pf_phase_idx, G, "pf_phase_idx") ||
+            !need(g.pf_floatfactor, 4 * (int64_t)G, "pf_floatfactor") ||
+            !need(g.pf_power2, G, "pf_power2") ||
+            !need(g.pf_approx_f32, g.pf_has_approx ? 2 * (int64_t)G : 0, "pf_approx_f32"))
+            return KSIM_ERR_MALFORMED_PROGRAM;
+
+        GraphDir &gd = img.gdir[k];
+        gd.G = G;
+        gd.P = P;
+        gd.stream_off = (int64_t)out.size();
+        std::vector<int64_t> &toff = img.term_off[k];
+        toff.reserve(G + 1);
+
+        for (int t = 0; t < G; ++t) {
+            const int64_t start = (int64_t)out.size();
+            toff.push_back(start);
+            // counts: the reference loops t < count, so a negative count is an
+            // empty loop; a count above the padded width would read another
+            // term's rows and is rejected.
+            int cnp = std::max(0, g.np_counts[t]);
+            int cph = std::max(0, g.ph_counts[t]);
+            if (cnp > g.Tnp || cph > g.Tph) {
+                err = gname + ": term " + std::to_string(t) + " count exceeds the padded width";
+                return KSIM_ERR_MALFORMED_PROGRAM;
+            }
+            std::vector<uint8_t> rec;  // column records of this term
+            double L = 0;              // log2 bound on max_k |sigma_k(z)| (z starts at 1)
+            double Lmax = 0;
+            const double kLim = 62.0 - 1e-9;
+            bool unsafe = false;
+            auto step = [&](double transient) {
+                Lmax = std::max(Lmax, transient);
+                if (transient > kLim) unsafe = true;
+            };
+            // NodePhases
+            uint32_t nu = 0;
+            int n_np = 0;
+            for (int c = 0; c < cnp; ++c) {
+                const size_t ci = (size_t)t * g.Tnp + c;
+                if (!pack_mask(g.np_params + ci * P, P, W, mask.data())) {
+                    err = gname + ": np_params holds a byte other than 0/1";
+                    return KSIM_ERR_MALFORMED_PROGRAM;
+                }
+                const uint32_t phase = g.np_phases[ci] & 7u;
+                const uint32_t j = phase & 3u;
+                uint32_t red = 0;
+                if (j == 0) {
+                    step(L + 1.0);  // 2z before it is halved back
+                } else {
+                    nu += (j & 1u) ? 1u : 2u;
+                    L += (j & 1u) ? std::log2(2.0 * std::cos(M_PI / 8)) : 0.5;
+                    step(L);
+                    if (nu >= 4) {
+                        nu -= 4;
+                        red = 1;
+                        L -= 1.0;
+                    }
+                }
+                for (int w = 0; w < W; ++w) put64(rec, mask[w]);
+                put64(rec, phase | (red ? NP_REDUCE_BIT : 0u));
+                for (int w = W + 1; w < R1; ++w) put64(rec, 0);
+                ++n_np;
+            }
+            // HalfPi
+            int n_hp = 0;
+            for (int c = 0; c < g.Thp; ++c) {
+                const size_t ci = (size_t)t * g.Thp + c;
+                if (!pack_mask(g.hp_params + ci * P, P, W, mask.data())) {
+                    err = gname + ": hp_params holds a byte other than 0/1";
+                    return KSIM_ERR_MALFORMED_PROGRAM;
+                }
+                const uint32_t coeff = g.hp_coeffs[ci] & 7u;
+                if (coeff == 0 || all_zero(mask.data(), W)) continue;
+                for (int w = 0; w < W; ++w) put64(rec, mask[w]);
+                put64(rec, coeff);
+                for (int w = W + 1; w < R1; ++w) put64(rec, 0);
+                ++n_hp;
+            }
+            // PiProducts
+            int n_pp = 0;
+            for (int c = 0; c < g.Tpp; ++c) {
+                const size_t ci = (size_t)t * g.Tpp + c;
+                if (!pack_mask(g.pp_psi_p + ci * P, P, W, mask.data()) ||
+                    !pack_mask(g.pp_phi_p + ci * P, P, W, mask.data() + W)) {
+                    err = gname + ": pp params hold a byte other than 0/1";
+                    return KSIM_ERR_MALFORMED_PROGRAM;
+                }
+                const uint32_t pc = g.pp_psi_c[ci] & 1u, qc = g.pp_phi_c[ci] & 1u;
+                const bool psi0 = pc == 0 && all_zero(mask.data(), W);
+                const bool phi0 = qc == 0 && all_zero(mask.data() + W, W);
+                if (psi0 || phi0) continue;
+                for (int w = 0; w < 2 * W; ++w) put64(rec, mask[w]);
+                put64(rec, pc | (qc << 1));
+                for (int w = 2 * W + 1; w < R2; ++w) put64(rec, 0);
+                ++n_pp;
+            }
+            // PhasePairs
+            int n_ph = 0;
+            for (int c = 0; c < cph; ++c) {
+                const size_t ci = (size_t)t * g.Tph + c;
+                if (!pack_mask(g.ph_alpha_p + ci * P, P, W, mask.data()) ||
+                    !pack_mask(g.ph_beta_p + ci * P, P, W, mask.data() + W)) {
+                    err = gname + ": ph params hold a byte other than 0/1";
+                    return KSIM_ERR_MALFORMED_PROGRAM;
+                }
+                const uint32_t ac = g.ph_alpha[ci] & 7u, bc = g.ph_beta[ci] & 7u;
+                uint64_t cw = ac | (bc << 3);
+                double fmax = 0;
+                for (uint32_t combo = 0; combo < 4; ++combo) {
+                    int64_t f[4];
+                    phase_pair((int)(ac ^ ((combo & 1u) << 2)), (int)(bc ^ ((combo >> 1) << 2)), f);
+                    cw |= (uint64_t)zw_valuation(f) << (8 + 4 * combo);
+                    fmax = std::max(fmax, max_embed(f));
+                }
+                step(L + 2.0);  // partial sums of four rotated copies
+                L += fmax > 0 ? std::log2(fmax) + 1e-12 : 0.0;
+                step(L);
+                for (int w = 0; w < 2 * W; ++w) put64(rec, mask[w]);
+                put64(rec, cw);
+                for (int w = 2 * W + 1; w < R2; ++w) put64(rec, 0);
+                ++n_ph;
+            }
+            // prefactor
+            const int32_t *ff = g.pf_floatfactor + 4 * (size_t)t;
+            const int64_t ff64[4] = {ff[0], ff[1], ff[2], ff[3]};
+            const double S = std::fabs((double)ff[0]) + std::fabs((double)ff[1]) +
+                             std::fabs((double)ff[2]) + std::fabs((double)ff[3]);
+            if (S > 0) step(L + std::log2(S) + 1e-12);
+            if (n_np > 0xFFFF || n_hp > 0xFFFF || n_pp > 0xFFFF || n_ph > 0xFFFF) {
+                err = gname + ": a term has more than 65535 columns in one family";
+                return KSIM_ERR_UNSUPPORTED;
+            }
+            uint32_t flags = unsafe ? TF_SLOW : 0u;
+            if (g.pf_has_approx) flags |= TF_APX;
+            put32(out, (uint32_t)n_np | ((uint32_t)n_hp << 16));
+            put32(out, (uint32_t)n_pp | ((uint32_t)n_ph << 16));
+            put32(out, (g.pf_phase_idx[t] & 7u) | (nu << 8) | (flags << 16));
+            put32(out, (uint32_t)g.pf_power2[t]);
+            for (int i = 0; i < 4; ++i) put32(out, (uint32_t)ff[i]);
+            if (g.pf_has_approx) {
+                double ar = g.pf_approx_f32[2 * (size_t)t], ai = g.pf_approx_f32[2 * (size_t)t + 1];
+                uint64_t u;
+                std::memcpy(&u, &ar, 8);
+                put64(out, u);
+                std::memcpy(&u, &ai, 8);
+                put64(out, u);
+            }
+            out.insert(out.end(), rec.begin(), rec.end());
+            (void)ff64;
+            const int64_t tb = (int64_t)out.size() - start;
+            img.max_term_bytes = std::max(img.max_term_bytes, tb);
+            img.n_terms += 1;
+            img.n_slow_terms += unsafe ? 1 : 0;
+            img.n_columns += n_np + n_hp + n_pp + n_ph;
+        }
+        toff.push_back((int64_t)out.size());
+        gd.stream_bytes = (int64_t)out.size() - gd.stream_off;
+        gd.n_chunks = 0;
+        gd.first_chunk = 0;
+    }
+    std::memcpy(out.data(), img.gdir.data(), sizeof(GraphDir) * (size_t)n_graphs);
+    return KSIM_OK;
+}
+
+bool make_chunks(const HostImage &img, int64_t slot_bytes, std::vector<ChunkDir> &out)
+{
+    out.clear();
+    for (int k = 0; k < img.n_graphs; ++k) {
+        const std::vector<int64_t> &to = img.term_off[k];
+        const int G = (int)to.size() - 1;
+        if (G <= 0) {
+            ChunkDir c = {};
+            c.off = img.gdir[k].stream_off;
+            c.graph = k;
+            c.end_of_graph = 1;
+            out.push_back(c);
+            continue;
+        }
+        int t = 0;
+        while (t < G) {
+            ChunkDir c = {};
+            c.off = to[t];
+            c.graph = k;
+            int u = t;
+            while (u < G && to[u + 1] - c.off <= slot_bytes) ++u;
+            if (u == t) return false;  // a single term does not fit
+            c.bytes = (int32_t)(to[u] - c.off);
+            c.n_terms = u - t;
+            c.end_of_graph = (u == G) ? 1 : 0;
+            out.push_back(c);
+            t = u;
+        }
+    }
+    return true;
+}
+
+}  // namespace ksim

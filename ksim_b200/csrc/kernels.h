@@ -1,0 +1,56 @@
+// kernels.h — launch interface of the sm_100a kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "image.h"
+
+namespace ksim {
+
+// One sampling job: a component image, its input rows and output placement.
+struct SampleJob {
+    const uint8_t *image;      // device program image
+    const GraphDir *gdir;      // = image
+    const ChunkDir *cdir;      // device chunk directory for slot_bytes
+    int32_t n_chunks, n_graphs, F, n_out;
+    int32_t slot_bytes, rng_mode;
+    const uint8_t *f;          // rows of f bytes
+    int64_t f_stride;          // bytes between rows
+    const int32_t *f_sel;      // nullable: column j of the component = f[row][f_sel[j]]
+    uint8_t *out;              // output bytes
+    int64_t out_stride, out_col0;
+    const int32_t *out_cols;   // nullable: output i goes to column out_cols[i]
+    double *amp;               // nullable: (B, n_out+1) |A_k|
+    int64_t B, shot_offset;
+    uint64_t seed;
+    uint32_t *status;          // KSIM_FLAG_* accumulator
+};
+
+struct LaunchCfg {
+    int threads = 256;   // shots per CTA (one shot per thread)
+    int staged = 1;      // stage term chunks in shared memory with TMA bulk copies
+    int slot_bytes = 16384;
+};
+
+// Launch the plain (one component per launch) sampler.
+cudaError_t launch_sample(const SampleJob &job, int W, const LaunchCfg &cfg, cudaStream_t st);
+
+enum EvalMode { EVAL_COMPLEX = 0, EVAL_ABS = 1, EVAL_TERMS = 2 };
+
+struct EvalJob {
+    const uint8_t *image;
+    const GraphDir *gdir;
+    int32_t graph;
+    const uint8_t *params;   // (B, P) bytes
+    int64_t B, P;
+    int32_t mode;
+    void *out;               // complex: (B,2) f64; abs: (B,) f64; terms: (B,G,5) i64
+    uint32_t *status;
+};
+
+cudaError_t launch_eval(const EvalJob &job, int W, cudaStream_t st);
+
+// Shared-memory bytes the staged sampler needs for a slot size.
+size_t staged_smem_bytes(int slot_bytes);
+
+}  // namespace ksim

@@ -1,0 +1,75 @@
+// runtime.h — host-side objects behind the C ABI handles.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/ksim_b200.h"
+#include "image.h"
+#include "kernels.h"
+
+namespace ksim {
+
+ksim_status fail(ksim_status s, const std::string &m);
+ksim_status cuda_fail(cudaError_t e, const char *what);
+
+// Select a device for the lifetime of a call and restore the caller's.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = true;
+    explicit DeviceGuard(int dev);
+    ~DeviceGuard();
+};
+
+// Grow-only device workspace.
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t n);
+    void release();
+};
+
+struct ComponentChunks {
+    ChunkDir *d = nullptr;
+    int n = 0;
+};
+
+}  // namespace ksim
+
+struct ksim_component {
+    int device = 0;
+    ksim::HostImage img;  // directory and term offsets (packed bytes freed after upload)
+    uint8_t *d_image = nullptr;
+    size_t image_bytes = 0;
+    std::map<int, ksim::ComponentChunks> chunks;  // by staging slot size
+    uint32_t *d_status = nullptr;
+    cudaStream_t stream = nullptr;
+    ksim::DevBuf ws_f, ws_out, ws_aux;
+    ksim::LaunchCfg cfg;
+    std::mutex mu;
+};
+
+struct ProgramPart {
+    ksim_component *comp = nullptr;
+    int32_t *d_sel = nullptr;   // f_selection on the device
+    int32_t *d_cols = nullptr;  // destination output column of each component output
+};
+
+struct ksim_program {
+    int device = 0;
+    int n_outputs = 0;
+    int min_f_cols = 0;
+    std::vector<ProgramPart> parts;
+    cudaStream_t stream = nullptr;
+    ksim::DevBuf ws_f, ws_out;
+    std::mutex mu;
+};
+
+namespace ksim {
+ksim_status component_chunks(ksim_component *c, int slot_bytes, const ChunkDir **d, int *n);
+ksim_status component_job(ksim_component *c, const LaunchCfg &cfg, SampleJob &j);
+}  // namespace ksim

@@ -1,0 +1,502 @@
+// zring.cuh — exact Z[w] term evaluation over the packed program image.
+//
+// w = e^{i pi/4}.  Elements are (a, b, c, d) in the basis (1, w, i, conj w),
+// the representation of the reference (zx_eval.hpp:25-47), held as uint64 so
+// every add and multiply wraps exactly like the reference's int64.
+//
+// Multiplying by w^j is a signed rotation of the coefficients:
+//   w^0: ( a,  b,  c,  d)      w^1: ( d,  a,  b, -c)
+//   w^2: (-c,  d,  a, -b)      w^3: (-b, -c,  d, -a)      w^(j+4) = -w^j
+// so every family factor except the floatfactor is a few adds, not a 16-multiply
+// product:
+//   NodePhases  (1 + w^k), k = phase ^ 4*par  ->  z + s*R_j(z), s = +-1 per shot
+//   PhasePairs  1 + w^a + w^b - w^(a+b)        ->  z + sa*R(z) + sb*R(z) + sc*R(z)
+//   HalfPi / phase index: a rotation; PiProducts: a sign.
+//
+// Renormalisation ("halve when all four are even and not all zero",
+// zx_eval.hpp:35-41) is decided without looking at the coefficients: for
+// nonzero z, all four are even  <=>  nu(z) >= 4, where nu is the
+// (1 - w)-adic valuation (2 = unit * (1 - w)^4), and nu is additive under
+// products.  The NodePhases factors have nu = 1 (j odd), 2 (j = 2), 4 (j = 0,
+// value 2) or are zero, so within the NodePhases block the halving steps are
+// the same for every shot and the host precomputes them (bit 3 of the column
+// word).  PhasePairs factors depend on the shot's parities; their nu for each
+// of the four parity combinations is tabulated by the host in the column word
+// and tracked per shot.  This reproduces the reference's (a, b, c, d, pw)
+// exactly whenever no coefficient leaves the int64 range; the host proves
+// that per term from an embedding-norm bound (|coefficient| <= max_k
+// |sigma_k(z)|), and terms it cannot prove safe are evaluated by
+// eval_term_exact, the reference's step-by-step arithmetic including the
+// explicit evenness test and int64 wrap.
+#pragma once
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define KS_HD __host__ __device__ __forceinline__
+#else
+#define KS_HD inline
+#endif
+
+namespace ksim {
+
+// ---- image record layout (shared with image.cpp) --------------------------
+enum : uint32_t { TF_SLOW = 1u, TF_APX = 2u };
+constexpr int TERM_HDR_BYTES = 32;
+constexpr int TERM_APX_BYTES = 16;
+// NodePhases / HalfPi column: W mask words + 1 constant word, padded to 16 B
+KS_HD constexpr int rec1_words(int W) { return (W + 2) & ~1; }
+// PiProducts / PhasePairs column: 2W mask words + 1 constant word, padded
+KS_HD constexpr int rec2_words(int W) { return (2 * W + 2) & ~1; }
+constexpr uint32_t NP_REDUCE_BIT = 8u;
+constexpr uint32_t NU_ZERO = 15u;  // PhasePairs factor is exactly zero
+
+struct Zu { uint64_t a, b, c, d; };
+
+KS_HD uint64_t sneg(uint64_t x, uint64_t m) { return (x ^ m) - m; }  // m = 0: x, m = ~0: -x
+
+KS_HD uint32_t popc64(uint64_t x)
+{
+#if defined(__CUDA_ARCH__)
+    return (uint32_t)__popc((uint32_t)x ^ (uint32_t)(x >> 32));
+#else
+    return (uint32_t)__builtin_popcountll(x);
+#endif
+}
+
+template <int W>
+KS_HD uint32_t parity(const uint64_t *m, const uint64_t (&v)[W])
+{
+    uint64_t x = m[0] & v[0];
+#pragma unroll
+    for (int w = 1; w < W; ++w) x ^= m[w] & v[w];
+    return popc64(x) & 1u;
+}
+
+// IEEE double ops that the compiler may not contract into FMAs.
+KS_HD double dadd(double x, double y)
+{
+#if defined(__CUDA_ARCH__)
+    return __dadd_rn(x, y);
+#else
+    return x + y;
+#endif
+}
+KS_HD double dsub(double x, double y)
+{
+#if defined(__CUDA_ARCH__)
+    return __dsub_rn(x, y);
+#else
+    return x - y;
+#endif
+}
+KS_HD double dmul(double x, double y)
+{
+#if defined(__CUDA_ARCH__)
+    return __dmul_rn(x, y);
+#else
+    return x * y;
+#endif
+}
+KS_HD double bits_to_double(uint64_t u)
+{
+#if defined(__CUDA_ARCH__)
+    return __longlong_as_double((long long)u);
+#else
+    double d;
+    __builtin_memcpy(&d, &u, 8);
+    return d;
+#endif
+}
+
+// 2^n exactly (the value exp2 returns for an integer argument, including the
+// subnormal range and the 0 / +inf ends).
+KS_HD double pow2i(int64_t n)
+{
+    if (n > 1023) return bits_to_double(0x7FF0000000000000ull);
+    if (n >= -1022) return bits_to_double((uint64_t)(n + 1023) << 52);
+    if (n >= -1074) return bits_to_double(1ull << (n + 1074));
+    return 0.0;
+}
+
+// z * w^k for a per-shot k in 0..7 (selects, no branches).
+KS_HD Zu rot_var(Zu z, uint32_t k)
+{
+    const bool k1 = k & 1u, k2 = k & 2u;
+    Zu r;
+    r.a = k1 ? z.d : z.a;
+    r.b = k1 ? z.a : z.b;
+    r.c = k1 ? z.b : z.c;
+    r.d = k1 ? (0 - z.c) : z.d;
+    Zu q;
+    q.a = k2 ? (0 - r.c) : r.a;
+    q.b = k2 ? r.d : r.b;
+    q.c = k2 ? r.a : r.c;
+    q.d = k2 ? (0 - r.b) : r.d;
+    const uint64_t m = 0 - (uint64_t)((k >> 2) & 1u);
+    q.a = sneg(q.a, m); q.b = sneg(q.b, m); q.c = sneg(q.c, m); q.d = sneg(q.d, m);
+    return q;
+}
+
+// acc += s * R_j(t), s = +1 (m = 0) or -1 (m = ~0), j in 0..3 the same for all shots.
+KS_HD void add_rot(Zu &acc, const Zu &t, uint32_t j, uint64_t m)
+{
+    switch (j & 3u) {
+    case 0: acc.a += sneg(t.a, m); acc.b += sneg(t.b, m); acc.c += sneg(t.c, m); acc.d += sneg(t.d, m); break;
+    case 1: acc.a += sneg(t.d, m); acc.b += sneg(t.a, m); acc.c += sneg(t.b, m); acc.d -= sneg(t.c, m); break;
+    case 2: acc.a -= sneg(t.c, m); acc.b += sneg(t.d, m); acc.c += sneg(t.a, m); acc.d -= sneg(t.b, m); break;
+    default: acc.a -= sneg(t.b, m); acc.b -= sneg(t.c, m); acc.c += sneg(t.d, m); acc.d -= sneg(t.a, m); break;
+    }
+}
+
+// Full product (zx_eval.hpp:27-33 formula, basis (1, w, i, conj w)).
+KS_HD Zu zmul(const Zu &x, const Zu &y)
+{
+    Zu r;
+    r.a = x.a * y.a + x.b * y.d - x.c * y.c + x.d * y.b;
+    r.b = x.a * y.b + x.b * y.a + x.c * y.d + x.d * y.c;
+    r.c = x.a * y.c + x.b * y.b + x.c * y.a - x.d * y.d;
+    r.d = x.a * y.d - x.b * y.c - x.c * y.b + x.d * y.a;
+    return r;
+}
+
+KS_HD void shr1_all(Zu &z)
+{
+    z.a = (uint64_t)((int64_t)z.a >> 1);
+    z.b = (uint64_t)((int64_t)z.b >> 1);
+    z.c = (uint64_t)((int64_t)z.c >> 1);
+    z.d = (uint64_t)((int64_t)z.d >> 1);
+}
+
+// One renormalisation step with the explicit test (zx_eval.hpp:35-41).
+KS_HD void zreduce(Zu &z, int64_t &pw)
+{
+    const uint64_t o = z.a | z.b | z.c | z.d;
+    if (o != 0 && (o & 1u) == 0) {
+        shr1_all(z);
+        pw += 1;
+    }
+}
+
+KS_HD bool over62(const Zu &z)
+{
+    const uint64_t k = 1ull << 62, lim = 1ull << 63;
+    return (z.a + k) > lim || (z.b + k) > lim || (z.c + k) > lim || (z.d + k) > lim;
+}
+
+struct TermHdr {
+    uint32_t n_np, n_hp, n_pp, n_ph;
+    uint32_t pf_idx, nu_np, flags;
+    int32_t power2;
+    Zu ff;
+};
+
+KS_HD TermHdr load_hdr(const uint8_t *p)
+{
+    const uint32_t *u = (const uint32_t *)p;
+    const uint32_t w0 = u[0], w1 = u[1], w2 = u[2];
+    TermHdr h;
+    h.n_np = w0 & 0xFFFFu; h.n_hp = w0 >> 16;
+    h.n_pp = w1 & 0xFFFFu; h.n_ph = w1 >> 16;
+    h.pf_idx = w2 & 7u; h.nu_np = (w2 >> 8) & 0xFFu; h.flags = (w2 >> 16) & 0xFFu;
+    h.power2 = (int32_t)u[3];
+    const int32_t *ff = (const int32_t *)(p + 16);
+    h.ff.a = (uint64_t)(int64_t)ff[0]; h.ff.b = (uint64_t)(int64_t)ff[1];
+    h.ff.c = (uint64_t)(int64_t)ff[2]; h.ff.d = (uint64_t)(int64_t)ff[3];
+    return h;
+}
+
+KS_HD int term_bytes(const TermHdr &h, int W)
+{
+    return TERM_HDR_BYTES + ((h.flags & TF_APX) ? TERM_APX_BYTES : 0) +
+           8 * (rec1_words(W) * (int)(h.n_np + h.n_hp) + rec2_words(W) * (int)(h.n_pp + h.n_ph));
+}
+
+// Load R 64-bit words of a 16-byte aligned record with 16-byte vector loads.
+template <int R>
+KS_HD void load_rec(const uint64_t *rec, uint64_t (&r)[R])
+{
+#if defined(__CUDA_ARCH__)
+    const ulonglong2 *q = (const ulonglong2 *)rec;
+#pragma unroll
+    for (int i = 0; i < R / 2; ++i) {
+        ulonglong2 x = q[i];
+        r[2 * i] = x.x;
+        r[2 * i + 1] = x.y;
+    }
+#else
+    for (int i = 0; i < R; ++i) r[i] = rec[i];
+#endif
+}
+
+struct TermOut {
+    Zu z;
+    int64_t pw;
+    int32_t power2;
+    uint32_t risk;  // KSIM_FLAG_INT64_RISK raised by the exact path
+};
+
+// Fast path: exact when the host proved every coefficient stays below 2^62.
+template <int W>
+KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const uint64_t (&v)[W],
+                                    TermOut &o)
+{
+    constexpr int R1 = rec1_words(W), R2 = rec2_words(W);
+    const uint64_t *q = (const uint64_t *)(p + TERM_HDR_BYTES + ((h.flags & TF_APX) ? TERM_APX_BYTES : 0));
+    Zu z = {1, 0, 0, 0};
+    int64_t pw = 0;
+    uint32_t alive = 1;
+
+    // NodePhases
+    for (uint32_t t = 0; t < h.n_np; ++t, q += R1) {
+        uint64_t r[R1];
+        load_rec<R1>(q, r);
+        uint64_t mw[W];
+#pragma unroll
+        for (int w = 0; w < W; ++w) mw[w] = r[w];
+        const uint32_t cw = (uint32_t)r[W];
+        const uint32_t neg = (parity<W>(mw, v) ^ (cw >> 2)) & 1u;
+        const uint32_t j = cw & 3u;
+        if (j == 0) {
+            // factor 2 (halved straight back, pw + 1) or 0 (the term dies)
+            pw += alive & (neg ^ 1u);
+            alive &= neg ^ 1u;
+            const uint64_t keep = 0 - (uint64_t)alive;
+            z.a &= keep; z.b &= keep; z.c &= keep; z.d &= keep;
+        } else {
+            const Zu t0 = z;
+            add_rot(z, t0, j, 0 - (uint64_t)neg);
+            if (cw & NP_REDUCE_BIT) {
+                shr1_all(z);
+                pw += alive;
+            }
+        }
+    }
+    // HalfPi: w^(sum par*coeff); its renormalisation cannot fire (nu < 4 here)
+    {
+        uint32_t tot = 0;
+        for (uint32_t t = 0; t < h.n_hp; ++t, q += R1) {
+            uint64_t r[R1];
+            load_rec<R1>(q, r);
+            uint64_t mw[W];
+#pragma unroll
+            for (int w = 0; w < W; ++w) mw[w] = r[w];
+            tot += parity<W>(mw, v) ? (uint32_t)r[W] : 0u;
+        }
+        z = rot_var(z, tot & 7u);
+    }
+    // PiProducts: overall sign
+    {
+        uint32_t e = 0;
+        for (uint32_t t = 0; t < h.n_pp; ++t, q += R2) {
+            uint64_t r[R2];
+            load_rec<R2>(q, r);
+            uint64_t ma[W], mb[W];
+#pragma unroll
+            for (int w = 0; w < W; ++w) { ma[w] = r[w]; mb[w] = r[W + w]; }
+            const uint32_t cw = (uint32_t)r[2 * W];
+            const uint32_t psi = (cw ^ parity<W>(ma, v)) & 1u;
+            const uint32_t phi = ((cw >> 1) ^ parity<W>(mb, v)) & 1u;
+            e ^= psi & phi;
+        }
+        const uint64_t m = 0 - (uint64_t)e;
+        z.a = sneg(z.a, m); z.b = sneg(z.b, m); z.c = sneg(z.c, m); z.d = sneg(z.d, m);
+    }
+    // PhasePairs: per-shot valuation tracking
+    {
+        uint32_t nu = h.nu_np;
+        for (uint32_t t = 0; t < h.n_ph; ++t, q += R2) {
+            uint64_t r[R2];
+            load_rec<R2>(q, r);
+            uint64_t ma[W], mb[W];
+#pragma unroll
+            for (int w = 0; w < W; ++w) { ma[w] = r[w]; mb[w] = r[W + w]; }
+            const uint32_t cw = (uint32_t)r[2 * W];
+            const uint32_t pa = parity<W>(ma, v), pb = parity<W>(mb, v);
+            const uint32_t ac = cw & 7u, bc = (cw >> 3) & 7u, gc = (ac + bc) & 7u;
+            const Zu t0 = z;
+            add_rot(z, t0, ac & 3u, 0 - (uint64_t)(((ac >> 2) ^ pa) & 1u));
+            add_rot(z, t0, bc & 3u, 0 - (uint64_t)(((bc >> 2) ^ pb) & 1u));
+            add_rot(z, t0, gc & 3u, 0 - (uint64_t)(((gc >> 2) ^ pa ^ pb ^ 1u) & 1u));
+            const uint32_t nf = (cw >> (8 + 4 * (pa | (pb << 1)))) & 15u;
+            alive &= (nf != NU_ZERO) ? 1u : 0u;
+            nu += nf;
+            const uint32_t red = alive & (nu >= 4 ? 1u : 0u);
+            nu -= 4 * red;
+            z.a = (uint64_t)((int64_t)z.a >> red);
+            z.b = (uint64_t)((int64_t)z.b >> red);
+            z.c = (uint64_t)((int64_t)z.c >> red);
+            z.d = (uint64_t)((int64_t)z.d >> red);
+            pw += red;
+        }
+    }
+    // prefactor: w^idx, then the exact floatfactor with one renormalisation
+    z = rot_var(z, h.pf_idx);
+    z = zmul(z, h.ff);
+    zreduce(z, pw);
+    o.z = z;
+    o.pw = pw;
+    o.power2 = h.power2;
+    o.risk = 0;
+    return (const uint8_t *)q;
+}
+
+// Exact path: the reference's step-by-step arithmetic (zx_eval.hpp:101-165),
+// int64 wrap included, over the same records.
+template <int W>
+KS_HD const uint8_t *eval_term_exact(const uint8_t *p, const TermHdr &h, const uint64_t (&v)[W],
+                                     TermOut &o)
+{
+    constexpr int R1 = rec1_words(W), R2 = rec2_words(W);
+    const uint64_t *q = (const uint64_t *)(p + TERM_HDR_BYTES + ((h.flags & TF_APX) ? TERM_APX_BYTES : 0));
+    const Zu one = {1, 0, 0, 0};
+    Zu z = one;
+    int64_t pw = 0;
+    uint32_t risk = 0;
+    for (uint32_t t = 0; t < h.n_np; ++t, q += R1) {
+        const uint32_t cw = (uint32_t)q[W];
+        const uint32_t k = ((parity<W>(q, v) << 2) + (cw & 7u)) & 7u;
+        Zu u = rot_var(one, k);
+        u.a += 1;
+        risk |= over62(z);
+        z = zmul(z, u);
+        zreduce(z, pw);
+    }
+    {
+        uint32_t tot = 0;
+        for (uint32_t t = 0; t < h.n_hp; ++t, q += R1)
+            tot += (parity<W>(q, v) * (uint32_t)q[W]) & 7u;
+        risk |= over62(z);
+        z = zmul(z, rot_var(one, tot & 7u));
+        zreduce(z, pw);
+    }
+    {
+        uint32_t e = 0;
+        for (uint32_t t = 0; t < h.n_pp; ++t, q += R2) {
+            const uint32_t cw = (uint32_t)q[2 * W];
+            const uint32_t psi = (cw + parity<W>(q, v)) & 1u;
+            const uint32_t phi = ((cw >> 1) + parity<W>(q + W, v)) & 1u;
+            e ^= psi & phi;
+        }
+        if (e) { z.a = 0 - z.a; z.b = 0 - z.b; z.c = 0 - z.c; z.d = 0 - z.d; }
+    }
+    for (uint32_t t = 0; t < h.n_ph; ++t, q += R2) {
+        const uint32_t cw = (uint32_t)q[2 * W];
+        const uint32_t al = ((cw & 7u) + 4u * parity<W>(q, v)) & 7u;
+        const uint32_t be = (((cw >> 3) & 7u) + 4u * parity<W>(q + W, v)) & 7u;
+        const Zu u = rot_var(one, al), x = rot_var(one, be), y = rot_var(one, (al + be) & 7u);
+        Zu term = {1 + u.a + x.a - y.a, u.b + x.b - y.b, u.c + x.c - y.c, u.d + x.d - y.d};
+        risk |= over62(z);
+        z = zmul(z, term);
+        zreduce(z, pw);
+    }
+    risk |= over62(z);
+    z = zmul(z, rot_var(one, h.pf_idx));
+    risk |= over62(z);
+    z = zmul(z, h.ff);
+    zreduce(z, pw);
+    o.z = z;
+    o.pw = pw;
+    o.power2 = h.power2;
+    o.risk = risk ? 1u : 0u;
+    return (const uint8_t *)q;
+}
+
+constexpr double SQ = 0.70710678118654752440;  // cos(pi/4)
+
+// Complex value of a finished term (zx_eval.hpp:166-176), no FMA contraction.
+KS_HD void term_complex(const TermOut &o, const uint8_t *hdr_ptr, uint32_t flags, double &re, double &im)
+{
+    const double A = (double)(int64_t)o.z.a, Bv = (double)(int64_t)o.z.b;
+    const double C = (double)(int64_t)o.z.c, D = (double)(int64_t)o.z.d;
+    re = dadd(A, dmul(dadd(Bv, D), SQ));
+    im = dadd(C, dmul(dsub(Bv, D), SQ));
+    const double s = pow2i(o.pw + (int64_t)o.power2);
+    re = dmul(re, s);
+    im = dmul(im, s);
+    if (flags & TF_APX) {
+        const double *ap = (const double *)(hdr_ptr + TERM_HDR_BYTES);
+        const double ar = ap[0], ai = ap[1];
+        const double r2 = dsub(dmul(re, ar), dmul(im, ai));
+        im = dadd(dmul(re, ai), dmul(im, ar));
+        re = r2;
+    }
+}
+
+// Evaluate `n_terms` consecutive term records starting at p, adding their
+// complex values to (sum_re, sum_im) in order.  Returns the end pointer.
+template <int W>
+KS_HD const uint8_t *eval_terms(const uint8_t *p, uint32_t n_terms, const uint64_t (&v)[W],
+                                double &sum_re, double &sum_im, uint32_t &risk)
+{
+    for (uint32_t t = 0; t < n_terms; ++t) {
+        const TermHdr h = load_hdr(p);
+        TermOut o;
+        const uint8_t *next = (h.flags & TF_SLOW) ? eval_term_exact<W>(p, h, v, o)
+                                                  : eval_term_fast<W>(p, h, v, o);
+        double re, im;
+        term_complex(o, p, h.flags, re, im);
+        sum_re = dadd(sum_re, re);
+        sum_im = dadd(sum_im, im);
+        risk |= o.risk;
+        p = next;
+    }
+    return p;
+}
+
+// Parameter-vector masks: bits [lo, hi) of word w.
+KS_HD uint64_t bit_range(int w, int64_t lo, int64_t hi)
+{
+    const int64_t b0 = (int64_t)w * 64, b1 = b0 + 64;
+    const int64_t s = lo > b0 ? lo : b0, e = hi < b1 ? hi : b1;
+    if (e <= s) return 0;
+    const int n = (int)(e - s), o = (int)(s - b0);
+    const uint64_t m = n == 64 ? ~0ull : ((1ull << n) - 1);
+    return m << o;
+}
+
+// ---- uniform streams --------------------------------------------------------
+KS_HD uint64_t xorshift_init(uint64_t seed, uint64_t shot)
+{
+    uint64_t r = seed ^ (shot * 0x9e3779b97f4a7c15ull);
+    r ^= r >> 30;
+    r *= 0xbf58476d1ce4e5b9ull;
+    r ^= r >> 27;
+    return r ? r : 1ull;
+}
+
+KS_HD double xorshift_uniform(uint64_t &s)
+{
+    s ^= s << 13;
+    s ^= s >> 7;
+    s ^= s << 17;
+    return (double)(s >> 11) * (1.0 / 9007199254740992.0);
+}
+
+KS_HD uint32_t mulhi32(uint32_t a, uint32_t b)
+{
+#if defined(__CUDA_ARCH__)
+    return __umulhi(a, b);
+#else
+    return (uint32_t)(((uint64_t)a * b) >> 32);
+#endif
+}
+
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): 10 rounds of the
+// multiply-xor S-box with Weyl key schedule.
+KS_HD double philox_uniform(uint64_t seed, uint64_t shot, uint32_t output)
+{
+    uint32_t c0 = (uint32_t)shot, c1 = (uint32_t)(shot >> 32), c2 = output, c3 = 0;
+    uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        if (r) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+        const uint32_t h0 = mulhi32(0xD2511F53u, c0), l0 = 0xD2511F53u * c0;
+        const uint32_t h1 = mulhi32(0xCD9E8D57u, c2), l1 = 0xCD9E8D57u * c2;
+        const uint32_t n0 = h1 ^ c1 ^ k0, n2 = h0 ^ c3 ^ k1;
+        c0 = n0; c1 = l1; c2 = n2; c3 = l0;
+    }
+    const uint64_t bits = ((uint64_t)c1 << 32) | c0;
+    return (double)(bits >> 11) * (1.0 / 9007199254740992.0);
+}
+
+}  // namespace ksim

@@ -1,0 +1,82 @@
+"""``B200ProgramSampler`` — drop-in for the reference's ``KokkosProgramSampler``.
+
+``B200ProgramSampler(prog).sample(f_params, seed)`` has the signature and the
+result of ``KokkosProgramSampler`` (``src/python/ksim/sample/sampler.py:46-67``)
+and of the numpy ``sample_flat`` (``sample/evaluate.py:69-87``): one native
+component per ``FlatComponent``, component ``k`` seeded with
+``seed + 0x9E37*k``, outputs concatenated and permuted by
+``argsort(output_order)``.  Here the f_selection gather, every component's
+kernel and the permutation run on the device in one native call.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _abi
+from ._abi import RNG_PHILOX, RNG_XORSHIFT, check, lib
+from .kokkos_sim import Component, _as_u64
+from .program import graph_to_dict
+
+__all__ = ["B200ProgramSampler", "KokkosProgramSampler", "graph_to_dict"]
+
+
+class B200ProgramSampler:
+    """GPU sampler for a FlatProgram (any object with the FlatProgram fields)."""
+
+    def __init__(self, prog, device: int = -1):
+        L = lib()
+        self.prog = prog
+        self.components = []
+        sels = []
+        for comp in prog.components:
+            sel = np.ascontiguousarray(np.asarray(comp.f_selection), dtype=np.int32).reshape(-1)
+            kc = Component([graph_to_dict(g) for g in comp.graphs], int(sel.shape[0]),
+                           device=device)
+            self.components.append((comp, kc))
+            sels.append(sel)
+        self._sels = sels
+        order = np.ascontiguousarray(np.asarray(prog.output_order), dtype=np.int32).reshape(-1)
+        self._order = order
+        n = len(self.components)
+        handles = (ctypes.c_void_p * max(n, 1))(*[kc.handle.value for _, kc in self.components])
+        sel_ptrs = (ctypes.POINTER(ctypes.c_int32) * max(n, 1))(*[_abi.i32ptr(s) for s in sels])
+        sel_len = np.array([s.shape[0] for s in sels] or [0], np.int32)
+        h = ctypes.c_void_p()
+        check(L.ksim_program_create(handles, n, sel_ptrs, _abi.i32ptr(sel_len), _abi.i32ptr(order),
+                                    int(order.shape[0]), ctypes.byref(h)))
+        self._h = h
+        self._L = L
+        self.num_outputs = int(order.shape[0])
+        self.min_f_cols = int(L.ksim_program_min_f_cols(h))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._L.ksim_program_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    def sample(self, f_params: np.ndarray, seed: int, rng_mode: int = RNG_XORSHIFT) -> np.ndarray:
+        f = np.ascontiguousarray(f_params, dtype=np.uint8)
+        if f.ndim != 2:
+            raise ValueError("f_params must be 2-D (shots, f parameters)")
+        B = f.shape[0]
+        s = _as_u64(seed)
+        _as_u64(s + 0x9E37 * max(len(self.components) - 1, 0))  # per-component seeds stay uint64
+        if f.shape[1] < self.min_f_cols:
+            raise IndexError(f"f_params has {f.shape[1]} columns; f_selection needs "
+                             f"{self.min_f_cols}")
+        out = np.zeros((B, self.num_outputs), np.uint8)
+        if B == 0 or self.num_outputs == 0:
+            return out
+        check(self._L.ksim_program_sample(self._h, _abi.u8ptr(f), B, f.shape[1], s, int(rng_mode),
+                                          _abi.u8ptr(out)))
+        return out
+
+
+KokkosProgramSampler = B200ProgramSampler

@@ -1,0 +1,154 @@
+// hostemu.cpp — TEST INFRASTRUCTURE ONLY.
+//
+// Runs the device term evaluator (ksim_b200/csrc/zring.cuh) on the CPU over
+// the packed image (ksim_b200/csrc/image.cpp), so the tests can check the
+// packing, the valuation-scheduled renormalisation and the overflow-safety
+// split against the oracle without a GPU.  It is never loaded by the
+// package; tests/conftest.py builds it with g++.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "image.h"
+#include "zring.cuh"
+
+using namespace ksim;
+
+namespace {
+std::string g_err;
+
+template <int W>
+void pack_row(const uint8_t *row, int64_t n, uint64_t (&v)[W])
+{
+    for (int w = 0; w < W; ++w) v[w] = 0;
+    for (int64_t c = 0; c < n && c < 64 * W; ++c) v[c >> 6] |= (uint64_t)(row[c] & 1u) << (c & 63);
+}
+
+template <int W>
+void eval_rows(const HostImage &img, int gi, const uint8_t *params, int64_t B, int64_t P, int mode,
+               void *out, uint32_t *risk_out)
+{
+    const GraphDir &gd = img.gdir[gi];
+    uint32_t risk = 0;
+    for (int64_t s = 0; s < B; ++s) {
+        uint64_t v[W];
+        pack_row<W>(params + s * P, P, v);
+        const uint8_t *p = img.bytes.data() + gd.stream_off;
+        if (mode == 2) {
+            int64_t *o = (int64_t *)out + s * (int64_t)gd.G * 5;
+            for (int t = 0; t < gd.G; ++t) {
+                const TermHdr h = load_hdr(p);
+                TermOut r;
+                p = (h.flags & TF_SLOW) ? eval_term_exact<W>(p, h, v, r) : eval_term_fast<W>(p, h, v, r);
+                o[5 * t] = (int64_t)r.z.a;
+                o[5 * t + 1] = (int64_t)r.z.b;
+                o[5 * t + 2] = (int64_t)r.z.c;
+                o[5 * t + 3] = (int64_t)r.z.d;
+                o[5 * t + 4] = r.pw;
+                risk |= r.risk;
+            }
+        } else {
+            double re = 0, im = 0;
+            eval_terms<W>(p, (uint32_t)gd.G, v, re, im, risk);
+            ((double *)out)[2 * s] = re;
+            ((double *)out)[2 * s + 1] = im;
+        }
+    }
+    if (risk_out) *risk_out = risk;
+}
+
+template <int W>
+void sample_rows(const HostImage &img, const uint8_t *f, int64_t B, uint64_t seed, int rng_mode, uint8_t *out,
+                 double *amp)
+{
+    const int F = img.F, n_out = img.n_out, ncol = n_out > 1 ? n_out : 1;
+    for (int64_t s = 0; s < B; ++s) {
+        uint64_t v[W];
+        pack_row<W>(f + s * F, F, v);
+        uint64_t rng = xorshift_init(seed, (uint64_t)s);
+        double prev = 0;
+        for (int k = 0; k < img.n_graphs; ++k) {
+            const int nm = k > 0 ? k - 1 : 0;
+            uint64_t vk[W];
+            for (int w = 0; w < W; ++w)
+                vk[w] = (v[w] & bit_range(w, 0, F + nm)) | (k > 0 ? bit_range(w, F + nm, img.gdir[k].P) : 0);
+            double re = 0, im = 0;
+            uint32_t risk = 0;
+            eval_terms<W>(img.bytes.data() + img.gdir[k].stream_off, (uint32_t)img.gdir[k].G, vk, re, im, risk);
+            const double mag = std::sqrt(re * re + im * im);
+            if (amp) amp[s * (n_out + 1) + k] = mag;
+            if (k == 0) {
+                prev = mag;
+                continue;
+            }
+            const int i = k - 1;
+            const double u = rng_mode == 1 ? philox_uniform(seed, (uint64_t)s, (uint32_t)i) : xorshift_uniform(rng);
+            const int bit = u < (mag / prev) ? 1 : 0;
+            v[(F + i) >> 6] |= (uint64_t)bit << ((F + i) & 63);
+            out[s * ncol + i] = (uint8_t)bit;
+            prev = bit ? mag : prev - mag;
+        }
+    }
+}
+
+#define DISPATCH(W, CALL)                \
+    switch (W) {                         \
+    case 1: CALL(1); break;              \
+    case 2: CALL(2); break;              \
+    case 3: CALL(3); break;              \
+    case 4: CALL(4); break;              \
+    case 5: CALL(5); break;              \
+    case 6: CALL(6); break;              \
+    case 8: CALL(8); break;              \
+    case 10: CALL(10); break;            \
+    case 12: CALL(12); break;            \
+    case 16: CALL(16); break;            \
+    default: return 99;                  \
+    }
+}  // namespace
+
+extern "C" {
+
+const char *hostemu_error(void) { return g_err.c_str(); }
+
+// stats: [W, n_terms, n_slow_terms, n_columns, max_term_bytes]
+int hostemu_stats(const ksim_graph_desc *g, int n, int F, int64_t *stats)
+{
+    HostImage img;
+    int st = build_image(g, n, F, img, g_err);
+    if (st) return st;
+    stats[0] = img.W;
+    stats[1] = img.n_terms;
+    stats[2] = img.n_slow_terms;
+    stats[3] = img.n_columns;
+    stats[4] = img.max_term_bytes;
+    return 0;
+}
+
+int hostemu_eval(const ksim_graph_desc *g, int n, int F, int gi, const uint8_t *params, int64_t B, int64_t P,
+                 int mode, void *out, uint32_t *risk)
+{
+    HostImage img;
+    int st = build_image(g, n, F, img, g_err);
+    if (st) return st;
+#define CALL_EVAL(WW) eval_rows<WW>(img, gi, params, B, P, mode, out, risk)
+    DISPATCH(img.W, CALL_EVAL)
+    return 0;
+}
+
+int hostemu_sample(const ksim_graph_desc *g, int n, int F, const uint8_t *f, int64_t B, uint64_t seed,
+                   int rng_mode, uint8_t *out, double *amp)
+{
+    HostImage img;
+    int st = build_image(g, n, F, img, g_err);
+    if (st) return st;
+#define CALL_SAMPLE(WW) sample_rows<WW>(img, f, B, seed, rng_mode, out, amp)
+    DISPATCH(img.W, CALL_SAMPLE)
+    return 0;
+}
+
+uint32_t hostemu_valuation(const int64_t *z) { return zw_valuation(z); }
+
+}  // extern "C"
