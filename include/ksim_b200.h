@@ -187,6 +187,57 @@ ksim_status ksim_program_sample_device(ksim_program *p, const uint8_t *d_f_param
                                        int64_t n_f_cols, int64_t shot_offset, uint64_t seed,
                                        int32_t rng_mode, uint8_t *d_out, void *stream);
 
+/* ---- batch: many programs in one persistent, graph-captured launch ------- */
+
+/* One sampling job of a batch: a component over device rows of f bytes,
+ * writing its outputs into device rows.  d_f_sel (nullable): component
+ * parameter j reads row[d_f_sel[j]]; d_out_cols (nullable): output i goes to
+ * column d_out_cols[i], else to out_col0 + i.  Shot s uses stream index
+ * shot_offset + s, so a job's bits do not depend on what else is batched. */
+typedef struct ksim_batch_job {
+    ksim_component *comp;
+    const uint8_t *d_f;
+    int64_t f_stride;
+    const int32_t *d_f_sel;
+    uint8_t *d_out;
+    int64_t out_stride, out_col0;
+    const int32_t *d_out_cols;
+    int64_t B, shot_offset;
+    uint64_t seed;
+    int32_t rng_mode;
+} ksim_batch_job;
+
+/* Launch shape of a batch (zero / negative fields take the defaults:
+ * 256 threads, 16 KiB slots, CTAs per SM from occupancy, graph on). */
+typedef struct ksim_batch_tuning {
+    int32_t threads;      /* shots per work item (one per thread), multiple of 32, <= 256 */
+    int32_t slot_bytes;   /* staging slot, multiple of 16, >= every job's largest term */
+    int32_t ctas_per_sm;  /* persistent CTAs per SM (<= occupancy limit) */
+    int32_t use_graph;    /* 1: capture counter reset + kernels in a CUDA graph */
+} ksim_batch_tuning;
+
+typedef struct ksim_batch ksim_batch;
+
+/* Components are borrowed and must outlive the batch; buffers are the
+ * caller's.  No reference counterpart (the reference launches one component
+ * at a time, sampler.py:60-64). */
+ksim_status ksim_batch_create(const ksim_batch_job *jobs, int32_t n_jobs, const ksim_batch_tuning *tuning,
+                              ksim_batch **out);
+/* The batch job for component k of program p over device rows of the full f
+ * matrix (f_stride bytes per row) and of the program's output matrix
+ * (n_outputs bytes per row): f_selection gather, output permutation and the
+ * per-component seed seed + 0x9E37*k as in KokkosProgramSampler.sample. */
+ksim_status ksim_program_job(const ksim_program *p, int32_t k, const uint8_t *d_f, int64_t f_stride,
+                             uint8_t *d_out, int64_t B, int64_t shot_offset, uint64_t seed, int32_t rng_mode,
+                             ksim_batch_job *out);
+int32_t ksim_program_n_components(const ksim_program *p);
+/* Replace every job's seed (n_jobs values) before the next launch. */
+ksim_status ksim_batch_set_seeds(ksim_batch *b, const uint64_t *seeds);
+/* Enqueue the whole batch on `stream` (replays the captured graph). */
+ksim_status ksim_batch_launch(ksim_batch *b, void *stream);
+ksim_status ksim_batch_info(const ksim_batch *b, int64_t *n_items, int32_t *grid, int32_t *n_launches);
+void ksim_batch_destroy(ksim_batch *b);
+
 /* ---- measurement --------------------------------------------------------- */
 
 /* Integer-pipe throughput of this GPU for the sampler's instruction mix

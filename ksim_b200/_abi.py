@@ -55,6 +55,22 @@ class GraphDesc(ctypes.Structure):
     ]
 
 
+class BatchJob(ctypes.Structure):
+    """``ksim_batch_job``."""
+    _fields_ = [
+        ("comp", ctypes.c_void_p), ("d_f", ctypes.c_void_p), ("f_stride", ctypes.c_int64),
+        ("d_f_sel", ctypes.c_void_p), ("d_out", ctypes.c_void_p), ("out_stride", ctypes.c_int64),
+        ("out_col0", ctypes.c_int64), ("d_out_cols", ctypes.c_void_p), ("B", ctypes.c_int64),
+        ("shot_offset", ctypes.c_int64), ("seed", ctypes.c_uint64), ("rng_mode", ctypes.c_int32),
+    ]
+
+
+class BatchTuning(ctypes.Structure):
+    """``ksim_batch_tuning``."""
+    _fields_ = [("threads", ctypes.c_int32), ("slot_bytes", ctypes.c_int32),
+                ("ctas_per_sm", ctypes.c_int32), ("use_graph", ctypes.c_int32)]
+
+
 _U8_KEYS = ("np_phases", "np_params", "hp_coeffs", "hp_params", "pp_psi_c", "pp_psi_p",
             "pp_phi_c", "pp_phi_p", "ph_alpha", "ph_alpha_p", "ph_beta", "ph_beta_p",
             "pf_phase_idx")
@@ -183,6 +199,15 @@ def _declare(L: ctypes.CDLL) -> None:
         "ksim_program_sample": (i32, [vp, _u8p, i64, i64, u64, i32, _u8p]),
         "ksim_program_sample_device": (i32, [vp, vp, i64, i64, i64, u64, i32, vp, vp]),
         "ksim_measure_int_peak": (i32, [i32, dp, dp]),
+        "ksim_batch_create": (i32, [ctypes.POINTER(BatchJob), i32, ctypes.POINTER(BatchTuning),
+                                    ctypes.POINTER(vp)]),
+        "ksim_batch_set_seeds": (i32, [vp, ctypes.POINTER(u64)]),
+        "ksim_program_job": (i32, [vp, i32, vp, i64, vp, i64, i64, u64, i32,
+                                   ctypes.POINTER(BatchJob)]),
+        "ksim_program_n_components": (i32, [vp]),
+        "ksim_batch_launch": (i32, [vp, vp]),
+        "ksim_batch_info": (i32, [vp, i64p, ctypes.POINTER(i32), ctypes.POINTER(i32)]),
+        "ksim_batch_destroy": (None, [vp]),
     }
     for name, (res, args) in sigs.items():
         f = getattr(L, name)

@@ -61,6 +61,7 @@ void DevBuf::release()
 
 ksim_status component_chunks(ksim_component *c, int slot_bytes, const ChunkDir **d, int *n)
 {
+    std::lock_guard<std::mutex> lk(c->chunk_mu);
     auto it = c->chunks.find(slot_bytes);
     if (it == c->chunks.end()) {
         std::vector<ChunkDir> host;
@@ -486,6 +487,31 @@ void ksim_program_destroy(ksim_program *p)
 }
 
 int32_t ksim_program_n_outputs(const ksim_program *p) { return p ? p->n_outputs : -1; }
+int32_t ksim_program_n_components(const ksim_program *p) { return p ? (int32_t)p->parts.size() : -1; }
+
+ksim_status ksim_program_job(const ksim_program *p, int32_t k, const uint8_t *d_f, int64_t f_stride, uint8_t *d_out,
+                             int64_t B, int64_t shot_offset, uint64_t seed, int32_t rng_mode, ksim_batch_job *out)
+{
+    if (!p || !out || k < 0 || k >= (int32_t)p->parts.size())
+        return fail(KSIM_ERR_INVALID_ARGUMENT, "bad program / component index");
+    if (f_stride < p->min_f_cols) return fail(KSIM_ERR_INVALID_ARGUMENT, "f_stride below the f_selection width");
+    const ProgramPart &part = p->parts[k];
+    ksim_batch_job j = {};
+    j.comp = part.comp;
+    j.d_f = d_f;
+    j.f_stride = f_stride;
+    j.d_f_sel = part.d_sel;
+    j.d_out = d_out;
+    j.out_stride = p->n_outputs;
+    j.out_col0 = 0;
+    j.d_out_cols = part.d_cols;
+    j.B = B;
+    j.shot_offset = shot_offset;
+    j.seed = seed + 0x9E37ull * (uint64_t)k;
+    j.rng_mode = rng_mode;
+    *out = j;
+    return KSIM_OK;
+}
 int32_t ksim_program_min_f_cols(const ksim_program *p) { return p ? p->min_f_cols : -1; }
 
 ksim_status ksim_program_sample_device(ksim_program *p, const uint8_t *d_f_params, int64_t B, int64_t n_f_cols,

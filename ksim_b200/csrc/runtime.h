@@ -50,7 +50,8 @@ struct ksim_component {
     cudaStream_t stream = nullptr;
     ksim::DevBuf ws_f, ws_out, ws_aux;
     ksim::LaunchCfg cfg;
-    std::mutex mu;
+    std::mutex mu;        // workspaces and cfg
+    std::mutex chunk_mu;  // the chunk-directory map
 };
 
 struct ProgramPart {

@@ -1,0 +1,234 @@
+// sample_tile.cuh — the per-CTA sampling loop shared by the plain kernel
+// (one component per launch) and the persistent batched kernel.
+//
+// One thread per shot runs the autoregressive loop of kokkos_sim.cpp:214-230:
+// |A_0|, then for every output i, p1 = |A_{i+1}|, one uniform, bit = u < p1/prev,
+// prev = bit ? p1 : prev - p1.  All shots of the CTA walk the same graphs in
+// the same order, so the term tables are uniform across the CTA: they stream
+// chunk by chunk (whole terms, <= slot bytes) from HBM into a two-slot
+// shared-memory ring with TMA bulk copies (cp.async.bulk + mbarrier
+// complete_tx); the copy of chunk c+2 is in flight while chunk c+1 is
+// evaluated, and each warp reads a column record with one broadcast 16-byte
+// shared load.  The shot's parameter vector [f | m | trying] is W 64-bit
+// registers; a parity is AND + popcount.
+//
+// Every mbarrier wait is bounded.  A wait that runs out raises
+// KSIM_FLAG_WAIT_TIMEOUT; the CTA then waits (bounded again) for the copies it
+// issued and returns false without writing outputs.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "../../include/ksim_b200.h"
+#include "kernels.h"
+#include "zring.cuh"
+
+namespace ksim {
+
+constexpr int NSLOT = 2;
+constexpr int BAR_BYTES = 128;
+constexpr long long WAIT_LIMIT = 1ll << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void tma_bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+{
+    const uint32_t a = smem_u32(bar);
+    for (long long it = 0; it < WAIT_LIMIT; ++it) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+// Prepare the barriers of a CTA's staging ring (once per CTA).
+__device__ __forceinline__ void ring_init(uint64_t *bar)
+{
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < NSLOT; ++i) mbar_init(&bar[i], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ double dsqrt(double x) { return __dsqrt_rn(x); }
+
+// Bit access by position with masks only (an indexed form would move the
+// register array to local memory).
+template <int W>
+__device__ __forceinline__ void set_bit(uint64_t (&v)[W], int pos, uint32_t bit)
+{
+#pragma unroll
+    for (int w = 0; w < W; ++w) v[w] |= bit_range(w, pos, pos + (int)bit);
+}
+
+template <int W>
+__device__ __forceinline__ uint32_t get_bit(const uint64_t (&v)[W], int pos)
+{
+    uint64_t x = 0;
+#pragma unroll
+    for (int w = 0; w < W; ++w) x |= v[w] & bit_range(w, pos, pos + 1);
+    return x != 0 ? 1u : 0u;
+}
+
+// Parameter vector of graph k: [f | m_0..m_{nm-1}] and, for k >= 1, the
+// "trying" bit on every position from F+nm up to the graph's P
+// (kokkos_sim.cpp:10-14 / zx_eval.hpp:86-90).
+template <int W>
+__device__ __forceinline__ void graph_vector(uint64_t (&vk)[W], const uint64_t (&v)[W], int F, int k, int P)
+{
+    const int nm = k > 0 ? k - 1 : 0;
+    const int64_t lo = (int64_t)F + nm;
+#pragma unroll
+    for (int w = 0; w < W; ++w) vk[w] = (v[w] & bit_range(w, 0, lo)) | (k > 0 ? bit_range(w, lo, P) : 0ull);
+}
+
+// Issue the copy of chunk c of job j; gidx is its position in the CTA's
+// running chunk count (it picks the slot and the barrier phase).
+__device__ __forceinline__ void issue_chunk(const SampleJob &j, int c, uint32_t gidx, uint64_t *bar, uint8_t *slots)
+{
+    const ChunkDir d = j.cdir[c];
+    const int slot = (int)(gidx & (NSLOT - 1));
+    if (d.bytes > 0) {
+        mbar_arrive_expect_tx(&bar[slot], (uint32_t)d.bytes);
+        tma_bulk_g2s(slots + (size_t)slot * j.slot_bytes, j.image + d.off, (uint32_t)d.bytes, &bar[slot]);
+    } else {
+        mbar_arrive(&bar[slot]);
+    }
+}
+
+// Sample shots [s0, s0 + blockDim.x) of job j.  g is the CTA's running chunk
+// count (advanced by the job's chunk count).  Returns false after a wait
+// timeout (the CTA must then stop using the ring).
+template <int W, bool STAGED>
+__device__ __forceinline__ bool sample_tile(const SampleJob &j, const int64_t s0, uint64_t *bar, uint8_t *slots,
+                                            uint32_t &g)
+{
+    const int tid = threadIdx.x;
+    const int64_t s = s0 + tid;
+    const bool act = s < j.B;
+    const int F = j.F;
+
+    uint64_t v[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) v[w] = 0;
+    if (act) {
+        const uint8_t *row = j.f + s * j.f_stride;
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            const int lim = min(64, F - 64 * w);
+            uint64_t x = 0;
+            for (int b = 0; b < lim; ++b) {
+                const int c = 64 * w + b;
+                const int col = j.f_sel ? j.f_sel[c] : c;
+                x |= (uint64_t)(row[col] & 1u) << b;
+            }
+            v[w] = x;
+        }
+    }
+    uint64_t vk[W];
+    graph_vector<W>(vk, v, F, 0, j.gdir[0].P);
+    const uint64_t shot = (uint64_t)(j.shot_offset + s);
+    uint64_t rng = xorshift_init(j.seed, shot);
+    double prev = 0.0, sre = 0.0, sim = 0.0;
+    uint32_t flags = 0, risk = 0;
+    const int nch = j.n_chunks;
+
+    if (STAGED && tid == 0)
+        for (int c = 0; c < NSLOT && c < nch; ++c) issue_chunk(j, c, g + (uint32_t)c, bar, slots);
+
+    for (int c = 0; c < nch; ++c) {
+        const ChunkDir d = j.cdir[c];
+        const uint32_t gc = g + (uint32_t)c;
+        const uint8_t *p;
+        if (STAGED) {
+            const int slot = (int)(gc & (NSLOT - 1));
+            const bool ok = mbar_wait(&bar[slot], (gc / NSLOT) & 1u);
+            if (__syncthreads_or(!ok)) {
+                if (tid == 0) {
+                    atomicOr(j.status, (uint32_t)KSIM_FLAG_WAIT_TIMEOUT);
+                    mbar_wait(&bar[slot], (gc / NSLOT) & 1u);
+                    if (c + 1 < nch) mbar_wait(&bar[(gc + 1) & (NSLOT - 1)], ((gc + 1) / NSLOT) & 1u);
+                }
+                return false;
+            }
+            p = slots + (size_t)slot * j.slot_bytes;
+        } else {
+            p = j.image + d.off;
+        }
+        if (act) eval_terms<W>(p, (uint32_t)d.n_terms, vk, sre, sim, risk);
+        if (d.end_of_graph) {
+            const int k = d.graph;
+            if (act) {
+                const double mag = dsqrt(dadd(dmul(sre, sre), dmul(sim, sim)));
+                if (j.amp) j.amp[s * (int64_t)(j.n_out + 1) + k] = mag;
+                if (k == 0) {
+                    prev = mag;
+                } else {
+                    const int i = k - 1;
+                    const double u = j.rng_mode == KSIM_RNG_PHILOX ? philox_uniform(j.seed, shot, (uint32_t)i)
+                                                                   : xorshift_uniform(rng);
+                    const double ratio = __ddiv_rn(mag, prev);
+                    const uint32_t bit = u < ratio ? 1u : 0u;
+                    if (!(prev > 0.0)) flags |= KSIM_FLAG_PREV_NONPOSITIVE;
+                    if (ratio != ratio) flags |= KSIM_FLAG_NAN;
+                    set_bit<W>(v, F + i, bit);
+                    prev = bit ? mag : dsub(prev, mag);
+                }
+            }
+            sre = 0.0;
+            sim = 0.0;
+            if (k + 1 < j.n_graphs) graph_vector<W>(vk, v, F, k + 1, j.gdir[k + 1].P);
+        }
+        if (STAGED) {
+            __syncthreads();
+            if (tid == 0 && c + NSLOT < nch) issue_chunk(j, c + NSLOT, gc + NSLOT, bar, slots);
+        }
+    }
+    g += (uint32_t)nch;
+
+    if (act) {
+        uint8_t *orow = j.out + s * j.out_stride;
+        for (int i = 0; i < j.n_out; ++i) {
+            const int64_t col = j.out_cols ? (int64_t)j.out_cols[i] : j.out_col0 + i;
+            orow[col] = (uint8_t)get_bit<W>(v, F + i);
+        }
+        const uint32_t st = flags | (risk ? (uint32_t)KSIM_FLAG_INT64_RISK : 0u);
+        if (st) atomicOr(j.status, st);
+    }
+    return true;
+}
+
+}  // namespace ksim

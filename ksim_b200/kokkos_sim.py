@@ -23,6 +23,7 @@ import numpy as np
 
 from . import _abi
 from ._abi import RNG_PHILOX, RNG_XORSHIFT, check, lib
+from .program import graph_to_dict
 
 __all__ = ["Component", "RNG_XORSHIFT", "RNG_PHILOX"]
 
@@ -51,7 +52,8 @@ class Component:
 
     def __init__(self, graphs: list, num_f: int, device: int = -1):
         L = lib()
-        graphs = list(graphs)
+        # reference-style dicts (sampler.py:21-43 layout) or FlatScalarGraph objects
+        graphs = [g if isinstance(g, dict) else graph_to_dict(g) for g in graphs]
         _abi.graph_shapes_ok(graphs)
         descs, keep = _abi.graphs_to_descs(graphs)
         h = ctypes.c_void_p()

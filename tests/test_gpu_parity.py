@@ -31,7 +31,7 @@ def device_sample(comp, f, seed, mode, shot_offset=0):
     from ksim_b200 import _abi
     B = f.shape[0]
     n_out = comp.n_out
-    d_f = torch.from_numpy(np.ascontiguousarray(f, np.uint8).reshape(B, -1)).cuda()
+    d_f = torch.from_numpy(np.ascontiguousarray(f, np.uint8).copy()).cuda()
     d_out = torch.zeros((B, max(n_out, 1)), dtype=torch.uint8, device="cuda")
     d_amp = torch.zeros((B, n_out + 1), dtype=torch.float64, device="cuda")
     st = torch.cuda.current_stream().cuda_stream
@@ -109,7 +109,13 @@ def test_launch_shapes_agree(cuda_device, oracle_port):
 def test_exact_path_and_wrap_on_gpu(cuda_device, oracle_port):
     from ksim_b200._abi import FLAG_INT64_RISK
     rng = np.random.default_rng(250)
-    gs = [synth.random_graph(rng, 4, 20 + k, 250, 3, 3, 40) for k in range(4)]
+    gs = [synth.random_graph(rng, 3, 20 + k, 250, 3, 3, 40) for k in range(4)]
+    for g in gs:
+        # 250 factors (1 + w^(1+4 par)): |coefficients| grow ~5.8^(n/4) and wrap int64
+        g.np_phases[:] = 1
+        g.np_params[:] = 0
+        g.np_params[:, ::7, 0] = 1
+        g.np_counts[:] = 250
     comp = FlatComponent((0, 1, 2), np.arange(20, dtype=np.int32), gs)
     kc = _component(comp.graphs, 20)
     po = oracle_port.PortOracle(comp.graphs, 20)

@@ -42,15 +42,37 @@ def test_random_components(hostemu, oracle_port, seed):
 
 
 @pytest.mark.parametrize("Tnp,Tph", [(60, 10), (130, 20), (250, 40)])
-def test_long_terms_exact_path_and_wrap(hostemu, oracle_port, Tnp, Tph):
-    """Terms the host cannot prove overflow-free take the exact path; at
-    Tnp=250 coefficients wrap int64 and both sides wrap identically."""
+def test_long_terms_exact_path(hostemu, oracle_port, Tnp, Tph):
+    """Terms the host cannot prove overflow-free take the exact path."""
     rng = np.random.default_rng(Tnp)
     gs = [synth.random_graph(rng, 4, 20 + k, Tnp, 3, 3, Tph) for k in range(4)]
     comp = FlatComponent((0, 1, 2), np.arange(20, dtype=np.int32), gs)
     st = _check_component(hostemu, oracle_port, comp, 20, rng, B=32)
     if Tnp >= 250:
         assert st["slow_terms"] == st["terms"]
+
+
+def test_int64_wrap_is_reproduced_and_flagged(hostemu, oracle_port):
+    """A term of 250 (1 + w^(1+4 par)) factors overflows int64; the exact path
+    wraps exactly like the reference and raises the risk flag."""
+    import ctypes
+    rng = np.random.default_rng(250)
+    gs = [synth.random_graph(rng, 3, 20 + k, 250, 3, 3, 40) for k in range(4)]
+    for g in gs:
+        g.np_phases[:] = 1
+        g.np_params[:] = 0
+        g.np_params[:, ::7, 0] = 1
+        g.np_counts[:] = 250
+    comp = FlatComponent((0, 1, 2), np.arange(20, dtype=np.int32), gs)
+    _check_component(hostemu, oracle_port, comp, 20, rng, B=16)
+    he = HostEmu(hostemu, comp.graphs, 20)
+    pv = rng.integers(0, 2, size=(8, 21)).astype(np.uint8)
+    out = np.zeros((8, 2))
+    risk = ctypes.c_uint32(0)
+    assert hostemu.hostemu_eval(he.descs, 4, 20, 1, pv.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+                                8, 21, 0, out.ctypes.data, ctypes.addressof(risk)) == 0
+    assert risk.value == 1
+    assert np.abs(he.eval_terms(1, pv)[..., :4].astype(float)).max() > 2.0**62
 
 
 def test_edge_cases(hostemu, oracle_port):
