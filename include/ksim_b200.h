@@ -132,6 +132,32 @@ ksim_status ksim_component_sample_device(ksim_component *c, const uint8_t *d_f_s
                                          int64_t out_stride, int64_t out_col0,
                                          double *d_amp, void *stream);
 
+/* The same sampling as ksim_component_sample_device (same arguments, same
+ * bits, same |A_k|), for callers that cannot allocate device memory: code
+ * whose HBM belongs to another allocator or is reserved up front, or that must
+ * not take the device-wide synchronisation a cudaMalloc / cudaFree may cause
+ * in a latency-critical loop.  No reference counterpart: kokkos_sim always
+ * allocates its Views inside Component.sample.
+ *
+ * The call allocates nothing.  Its scratch (the kernel's status word and the
+ * staging chunk directory) is one fixed array of KSIM_NOALLOC_SCRATCH_BYTES in
+ * device memory, loaded with the library on every GPU that uses it and held
+ * until the process exits.  A component needing more than
+ * KSIM_NOALLOC_MAX_CHUNKS staging chunks is rejected with
+ * KSIM_ERR_UNSUPPORTED.  The first call on a device looks up the array's
+ * device address; make that first call before any stream capture.  Every call
+ * shares the array and leaves its contents behind (each call clears the status
+ * word and rewrites the directory on `stream` before its kernel), so calls
+ * that overlap on the GPU (other streams, other threads) race on it: issue
+ * them on one stream. */
+#define KSIM_NOALLOC_SCRATCH_BYTES 33024
+#define KSIM_NOALLOC_MAX_CHUNKS 1024
+ksim_status ksim_component_sample_device_noalloc(ksim_component *c, const uint8_t *d_f_sel,
+                                                 int64_t B, int64_t shot_offset, uint64_t seed,
+                                                 int32_t rng_mode, uint8_t *d_out,
+                                                 int64_t out_stride, int64_t out_col0,
+                                                 double *d_amp, void *stream);
+
 /* |amplitude| of graph `graph` for B explicit parameter rows (B, P) uint8.
  * Replaces Component.eval_abs, kokkos_sim.cpp:157-185.  Host buffers. */
 ksim_status ksim_component_eval_abs(ksim_component *c, int32_t graph, const uint8_t *params,

@@ -183,6 +183,8 @@ def _declare(L: ctypes.CDLL) -> None:
         "ksim_component_sample": (i32, [vp, _u8p, i64, u64, i32, _u8p]),
         "ksim_component_sample_device": (i32, [vp, vp, i64, i64, u64, i32, vp, i64, i64,
                                                vp, vp]),
+        "ksim_component_sample_device_noalloc": (i32, [vp, vp, i64, i64, u64, i32, vp, i64,
+                                                       i64, vp, vp]),
         "ksim_component_eval_abs": (i32, [vp, i32, _u8p, i64, i64, dp]),
         "ksim_component_eval": (i32, [vp, i32, _u8p, i64, i64, dp]),
         "ksim_component_eval_terms": (i32, [vp, i32, _u8p, i64, i64, i64p]),
