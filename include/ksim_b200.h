@@ -264,6 +264,69 @@ ksim_status ksim_batch_launch(ksim_batch *b, void *stream);
 ksim_status ksim_batch_info(const ksim_batch *b, int64_t *n_items, int32_t *grid, int32_t *n_launches);
 void ksim_batch_destroy(ksim_batch *b);
 
+/* ---- serving: continuous batching with a device-resident request loop ---- */
+
+/* No reference counterpart (kokkos_sim serves one synchronous call at a time,
+ * kokkos_sim.cpp:188-241).  A server owns one device arena for request
+ * buffers; a request is admitted, strictly in arrival order, once its HBM
+ * footprint (f rows + output rows), a request slot, job-table slots and ring
+ * room are free.  Admitted work is published to a device job ring that a
+ * persistent kernel drains tile by tile: requests that arrive while others
+ * run join the ring, and their tiles interleave with the running ones on the
+ * device.  The loop kernel exits after idle_us without work and is relaunched
+ * by the server's scheduler thread when work arrives.  Results depend only on
+ * (program, f, seed, rng_mode), never on what else is in flight.
+ * Programs are borrowed: keep them alive until their requests finish. */
+typedef struct ksim_server_config {
+    int32_t device;          /* < 0: the calling thread's current device            */
+    int64_t arena_bytes;     /* admission budget for request buffers (default 1 GiB) */
+    int32_t max_requests;    /* request slots in flight (default 1024)               */
+    int32_t max_jobs;        /* job-table slots in flight (default 4096)             */
+    int32_t threads;         /* shots per tile = threads per CTA (default 256)       */
+    int32_t slot_bytes;      /* staging slot of the loop kernel (default 16 KiB)     */
+    int32_t ctas_per_sm;     /* loop CTAs per SM (default: occupancy limit)          */
+    int32_t idle_us;         /* loop CTAs exit after this long without work (1000)   */
+} ksim_server_config;
+
+typedef struct ksim_server_stats {
+    int64_t submitted, completed, failed, cancelled;
+    int64_t shots_completed;
+    int64_t loop_launches;   /* launches of the device-resident loop kernel */
+    int64_t side_launches;   /* programs with > 256 parameter bits run as plain launches */
+    int64_t pending, in_flight;
+    int64_t arena_in_use, arena_capacity;
+} ksim_server_stats;
+
+typedef struct ksim_server ksim_server;
+
+/* cfg may be NULL (all defaults); zero / negative fields take the defaults. */
+ksim_status ksim_server_create(const ksim_server_config *cfg, ksim_server **out);
+/* Queue a request: B shots of program p over host rows f (B rows of
+ * n_f_cols bytes, f_row_stride bytes apart), seed and rng_mode as in
+ * ksim_program_sample; results go to host `out` (B x n_outputs bytes) when
+ * the request completes.  f and out must stay valid until then; page-locked
+ * buffers let the copies overlap.  A request larger than the whole arena is
+ * rejected with KSIM_ERR_OUT_OF_MEMORY. */
+ksim_status ksim_server_submit(ksim_server *s, ksim_program *p, const uint8_t *f, int64_t B,
+                               int64_t n_f_cols, int64_t f_row_stride, uint64_t seed,
+                               int32_t rng_mode, uint8_t *out, int64_t *request_id);
+/* Block until the request finishes (timeout_ms < 0: no limit; on expiry
+ * KSIM_ERR_TIMEOUT and the request stays queued).  Returns the request's own
+ * status (KSIM_ERR_CANCELLED, KSIM_ERR_TIMEOUT for a device wait that ran
+ * out, ...).  latency_s (nullable): submit -> results in `out`, seconds;
+ * done_time_s (nullable): completion time on the CLOCK_MONOTONIC clock.
+ * A finished request is forgotten once waited on. */
+ksim_status ksim_server_wait(ksim_server *s, int64_t request_id, int32_t timeout_ms,
+                             double *latency_s, double *done_time_s);
+/* done = 1 when finished (then ksim_server_wait returns at once). */
+ksim_status ksim_server_poll(ksim_server *s, int64_t request_id, int32_t *done);
+/* Cancel a request that has not been admitted yet (KSIM_ERR_NOT_FOUND for
+ * an unknown id, KSIM_ERR_INVALID_ARGUMENT once it is on the device). */
+ksim_status ksim_server_cancel(ksim_server *s, int64_t request_id);
+ksim_status ksim_server_get_stats(ksim_server *s, ksim_server_stats *out);
+/* Stop the loop, finish or cancel what is queued, free everything. */
+void ksim_server_destroy(ksim_server *s);
+
 /* ---- measurement --------------------------------------------------------- */
 
 /* Integer-pipe throughput of this GPU for the sampler's instruction mix

@@ -71,6 +71,21 @@ class BatchTuning(ctypes.Structure):
                 ("ctas_per_sm", ctypes.c_int32), ("use_graph", ctypes.c_int32)]
 
 
+class ServerConfig(ctypes.Structure):
+    """``ksim_server_config``."""
+    _fields_ = [("device", ctypes.c_int32), ("arena_bytes", ctypes.c_int64),
+                ("max_requests", ctypes.c_int32), ("max_jobs", ctypes.c_int32),
+                ("threads", ctypes.c_int32), ("slot_bytes", ctypes.c_int32),
+                ("ctas_per_sm", ctypes.c_int32), ("idle_us", ctypes.c_int32)]
+
+
+class ServerStats(ctypes.Structure):
+    """``ksim_server_stats``."""
+    _fields_ = [(n, ctypes.c_int64) for n in (
+        "submitted", "completed", "failed", "cancelled", "shots_completed", "loop_launches",
+        "side_launches", "pending", "in_flight", "arena_in_use", "arena_capacity")]
+
+
 _U8_KEYS = ("np_phases", "np_params", "hp_coeffs", "hp_params", "pp_psi_c", "pp_psi_p",
             "pp_phi_c", "pp_phi_p", "ph_alpha", "ph_alpha_p", "ph_beta", "ph_beta_p",
             "pf_phase_idx")
@@ -210,6 +225,13 @@ def _declare(L: ctypes.CDLL) -> None:
         "ksim_batch_launch": (i32, [vp, vp]),
         "ksim_batch_info": (i32, [vp, i64p, ctypes.POINTER(i32), ctypes.POINTER(i32)]),
         "ksim_batch_destroy": (None, [vp]),
+        "ksim_server_create": (i32, [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]),
+        "ksim_server_submit": (i32, [vp, vp, vp, i64, i64, i64, u64, i32, vp, i64p]),
+        "ksim_server_wait": (i32, [vp, i64, i32, dp, dp]),
+        "ksim_server_poll": (i32, [vp, i64, ctypes.POINTER(i32)]),
+        "ksim_server_cancel": (i32, [vp, i64]),
+        "ksim_server_get_stats": (i32, [vp, ctypes.POINTER(ServerStats)]),
+        "ksim_server_destroy": (None, [vp]),
     }
     for name, (res, args) in sigs.items():
         f = getattr(L, name)

@@ -15,6 +15,11 @@
 // Every mbarrier wait is bounded.  A wait that runs out raises
 // KSIM_FLAG_WAIT_TIMEOUT; the CTA then waits (bounded again) for the copies it
 // issued and returns false without writing outputs.
+//
+// CG = true reads every job-dependent array (directories, f rows, column
+// maps) with L2-only loads.  The serving loop needs that: its CTAs live
+// across requests, and a request's buffers may reuse memory an earlier
+// request of the same kernel lifetime read through this SM's L1.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -85,6 +90,37 @@ __device__ __forceinline__ void ring_init(uint64_t *bar)
 
 __device__ __forceinline__ double dsqrt(double x) { return __dsqrt_rn(x); }
 
+// Loads of job-dependent data: plain, or L2-only when CG (see above).
+template <bool CG, typename T>
+__device__ __forceinline__ T ldj(const T *p)
+{
+    if (CG) return __ldcg(p);
+    return *p;
+}
+
+template <bool CG>
+__device__ __forceinline__ ChunkDir ld_chunk(const ChunkDir *p)
+{
+    if (!CG) return *p;
+    const longlong2 *q = (const longlong2 *)p;
+    const longlong2 a = __ldcg(q), b = __ldcg(q + 1);
+    ChunkDir d;
+    d.off = a.x;
+    d.bytes = (int32_t)(uint32_t)a.y;
+    d.graph = (int32_t)(a.y >> 32);
+    d.n_terms = (int32_t)(uint32_t)b.x;
+    d.end_of_graph = (int32_t)(b.x >> 32);
+    d.pad0 = (int32_t)(uint32_t)b.y;
+    d.pad1 = (int32_t)(b.y >> 32);
+    return d;
+}
+
+template <bool CG>
+__device__ __forceinline__ int graph_params(const GraphDir *g)
+{
+    return CG ? __ldcg(&g->P) : g->P;
+}
+
 // Bit access by position with masks only (an indexed form would move the
 // register array to local memory).
 template <int W>
@@ -117,9 +153,10 @@ __device__ __forceinline__ void graph_vector(uint64_t (&vk)[W], const uint64_t (
 
 // Issue the copy of chunk c of job j; gidx is its position in the CTA's
 // running chunk count (it picks the slot and the barrier phase).
+template <bool CG>
 __device__ __forceinline__ void issue_chunk(const SampleJob &j, int c, uint32_t gidx, uint64_t *bar, uint8_t *slots)
 {
-    const ChunkDir d = j.cdir[c];
+    const ChunkDir d = ld_chunk<CG>(j.cdir + c);
     const int slot = (int)(gidx & (NSLOT - 1));
     if (d.bytes > 0) {
         mbar_arrive_expect_tx(&bar[slot], (uint32_t)d.bytes);
@@ -132,7 +169,7 @@ __device__ __forceinline__ void issue_chunk(const SampleJob &j, int c, uint32_t 
 // Sample shots [s0, s0 + blockDim.x) of job j.  g is the CTA's running chunk
 // count (advanced by the job's chunk count).  Returns false after a wait
 // timeout (the CTA must then stop using the ring).
-template <int W, bool STAGED>
+template <int W, bool STAGED, bool CG = false>
 __device__ __forceinline__ bool sample_tile(const SampleJob &j, const int64_t s0, uint64_t *bar, uint8_t *slots,
                                             uint32_t &g)
 {
@@ -152,14 +189,14 @@ __device__ __forceinline__ bool sample_tile(const SampleJob &j, const int64_t s0
             uint64_t x = 0;
             for (int b = 0; b < lim; ++b) {
                 const int c = 64 * w + b;
-                const int col = j.f_sel ? j.f_sel[c] : c;
-                x |= (uint64_t)(row[col] & 1u) << b;
+                const int col = j.f_sel ? ldj<CG>(j.f_sel + c) : c;
+                x |= (uint64_t)(ldj<CG>(row + col) & 1u) << b;
             }
             v[w] = x;
         }
     }
     uint64_t vk[W];
-    graph_vector<W>(vk, v, F, 0, j.gdir[0].P);
+    graph_vector<W>(vk, v, F, 0, graph_params<CG>(j.gdir));
     const uint64_t shot = (uint64_t)(j.shot_offset + s);
     uint64_t rng = xorshift_init(j.seed, shot);
     double prev = 0.0, sre = 0.0, sim = 0.0;
@@ -167,10 +204,10 @@ __device__ __forceinline__ bool sample_tile(const SampleJob &j, const int64_t s0
     const int nch = j.n_chunks;
 
     if (STAGED && tid == 0)
-        for (int c = 0; c < NSLOT && c < nch; ++c) issue_chunk(j, c, g + (uint32_t)c, bar, slots);
+        for (int c = 0; c < NSLOT && c < nch; ++c) issue_chunk<CG>(j, c, g + (uint32_t)c, bar, slots);
 
     for (int c = 0; c < nch; ++c) {
-        const ChunkDir d = j.cdir[c];
+        const ChunkDir d = ld_chunk<CG>(j.cdir + c);
         const uint32_t gc = g + (uint32_t)c;
         const uint8_t *p;
         if (STAGED) {
@@ -210,11 +247,11 @@ __device__ __forceinline__ bool sample_tile(const SampleJob &j, const int64_t s0
             }
             sre = 0.0;
             sim = 0.0;
-            if (k + 1 < j.n_graphs) graph_vector<W>(vk, v, F, k + 1, j.gdir[k + 1].P);
+            if (k + 1 < j.n_graphs) graph_vector<W>(vk, v, F, k + 1, graph_params<CG>(j.gdir + k + 1));
         }
         if (STAGED) {
             __syncthreads();
-            if (tid == 0 && c + NSLOT < nch) issue_chunk(j, c + NSLOT, gc + NSLOT, bar, slots);
+            if (tid == 0 && c + NSLOT < nch) issue_chunk<CG>(j, c + NSLOT, gc + NSLOT, bar, slots);
         }
     }
     g += (uint32_t)nch;
@@ -222,7 +259,7 @@ __device__ __forceinline__ bool sample_tile(const SampleJob &j, const int64_t s0
     if (act) {
         uint8_t *orow = j.out + s * j.out_stride;
         for (int i = 0; i < j.n_out; ++i) {
-            const int64_t col = j.out_cols ? (int64_t)j.out_cols[i] : j.out_col0 + i;
+            const int64_t col = j.out_cols ? (int64_t)ldj<CG>(j.out_cols + i) : j.out_col0 + i;
             orow[col] = (uint8_t)get_bit<W>(v, F + i);
         }
         const uint32_t st = flags | (risk ? (uint32_t)KSIM_FLAG_INT64_RISK : 0u);

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "image.h"
+#include "serve_sched.h"
 #include "zring.cuh"
 
 using namespace ksim;
@@ -150,5 +151,42 @@ int hostemu_sample(const ksim_graph_desc *g, int n, int F, const uint8_t *f, int
 }
 
 uint32_t hostemu_valuation(const int64_t *z) { return zw_valuation(z); }
+
+// The server's arena (serve_sched.h) driven by a script: ops[2i] = 0 allocates
+// ops[2i+1] bytes (result: offset or -1), ops[2i] = 1 releases the offset
+// returned by op number ops[2i+1] (result: 1 released, 0 refused).  state:
+// in_use, largest_free, free_blocks, live_blocks after the script.
+void hostemu_arena_run(int64_t capacity, int64_t align, const int64_t *ops, int n_ops, int64_t *results,
+                       int64_t *state)
+{
+    Arena a(capacity, align);
+    for (int i = 0; i < n_ops; ++i) {
+        if (ops[2 * i] == 0) {
+            results[i] = a.alloc(ops[2 * i + 1]);
+        } else {
+            const int64_t k = ops[2 * i + 1];
+            results[i] = (k >= 0 && k < i) ? (a.release(results[k]) ? 1 : 0) : 0;
+        }
+    }
+    state[0] = a.in_use();
+    state[1] = a.largest_free();
+    state[2] = a.free_blocks();
+    state[3] = a.live_blocks();
+}
+
+// admissible() for an arena with one live block of `used` bytes at offset 0.
+int hostemu_admissible(int64_t need_bytes, int need_jobs, int64_t need_ring, int64_t arena_cap, int64_t used,
+                       int req_free, int req_total, int job_free, int job_total, int64_t ring_cap,
+                       int64_t ring_in_flight)
+{
+    Arena a(arena_cap, 256);
+    if (used > 0) a.alloc(used);
+    SlotPool rq(req_total), jb(job_total);
+    for (int i = req_free; i < req_total; ++i) rq.take();
+    for (int i = job_free; i < job_total; ++i) jb.take();
+    const AdmitNeed n = {need_bytes, need_jobs, need_ring};
+    const AdmitState st = {&a, &rq, &jb, ring_cap, ring_in_flight};
+    return admissible(n, st);
+}
 
 }  // extern "C"
