@@ -273,8 +273,8 @@ void ksim_batch_destroy(ksim_batch *b);
  * room are free.  Admitted work is published to a device job ring that a
  * persistent kernel drains tile by tile: requests that arrive while others
  * run join the ring, and their tiles interleave with the running ones on the
- * device.  The loop kernel exits after idle_us without work and is relaunched
- * by the server's scheduler thread when work arrives.  Results depend only on
+ * device.  The loop kernel exits once no CTA has claimed work for idle_us and
+ * is relaunched (full grid) by the server's scheduler thread when work arrives.  Results depend only on
  * (program, f, seed, rng_mode), never on what else is in flight.
  * Programs are borrowed: keep them alive until their requests finish. */
 typedef struct ksim_server_config {
@@ -282,10 +282,11 @@ typedef struct ksim_server_config {
     int64_t arena_bytes;     /* admission budget for request buffers (default 1 GiB) */
     int32_t max_requests;    /* request slots in flight (default 1024)               */
     int32_t max_jobs;        /* job-table slots in flight (default 4096)             */
-    int32_t threads;         /* shots per tile = threads per CTA (default 256)       */
+    int32_t threads;         /* shots per tile = threads per CTA (default 128)       */
     int32_t slot_bytes;      /* staging slot of the loop kernel (default 16 KiB)     */
     int32_t ctas_per_sm;     /* loop CTAs per SM (default: occupancy limit)          */
-    int32_t idle_us;         /* loop CTAs exit after this long without work (1000)   */
+    int32_t idle_us;         /* the loop exits after the whole grid claimed no work
+                                for this long (default 2000)                         */
 } ksim_server_config;
 
 typedef struct ksim_server_stats {

@@ -12,8 +12,12 @@
 // decrements the request's job count; the one that finishes the request
 // writes the request's sequence number into a host-mapped flag after a
 // system-scope fence.  With nothing to claim, thread 0 backs off with
-// __nanosleep and the CTA leaves after idle_us (or when the stop word is
-// set): every wait in the loop is bounded.
+// __nanosleep.  Leaving is collective: a CTA gives up only when no CTA of
+// the grid has claimed a tile for idle_us (the claim time is shared in the
+// control block), and the first to give up raises an exit word that makes
+// every other CTA leave at its next claim, so the grid never shrinks while
+// the kernel runs; the scheduler relaunches a full grid when work arrives.
+// Every wait in the loop is bounded.
 //
 // Host side (ksim_server): submit() queues a request; one scheduler thread
 //   1. admits queued requests in arrival order by HBM footprint
@@ -70,8 +74,9 @@ struct ServeReqDev {
 
 struct ServeCtl {
     unsigned long long head;  // ring position of the first job that may have tiles left
-    int32_t stop;
-    int32_t pad;
+    long long last_claim_ns;  // globaltimer of the latest tile claim of any CTA
+    int32_t stop;             // set by the host at shutdown
+    int32_t exiting;          // set by the first CTA that leaves; cleared before each launch
 };
 
 namespace {
@@ -102,12 +107,12 @@ __global__ void __launch_bounds__(256) k_serve(ServeJob *jobs, ServeReqDev *reqs
     uint8_t *slots = smem + BAR_BYTES;
     ring_init(bar);
     uint32_t g = 0;
-    long long idle_since = -1;
+    const long long t_start = global_ns();
     unsigned backoff = 64;
     for (;;) {
         if (threadIdx.x == 0) {
             int slot = -1, tile = -1;
-            for (int scan = 0; scan < SERVE_SCAN; ++scan) {
+            for (int scan = 0; scan < SERVE_SCAN && !vload(&ctl->exiting); ++scan) {
                 const unsigned long long h = vload(&ctl->head);
                 const unsigned long long e = vload(ring + (h % (unsigned long long)ring_cap));
                 if ((uint32_t)(e >> 32) != (uint32_t)(h + 1)) break;  // not published yet
@@ -121,13 +126,15 @@ __global__ void __launch_bounds__(256) k_serve(ServeJob *jobs, ServeReqDev *reqs
                 atomicCAS(&ctl->head, h, h + 1);  // exhausted: move the head on
             }
             if (slot >= 0) {
-                idle_since = -1;
                 backoff = 64;
+                *(volatile long long *)&ctl->last_claim_ns = global_ns();
                 s_W = vload(&jobs[slot].W);
             } else {
                 const long long now = global_ns();
-                if (idle_since < 0) idle_since = now;
-                if (vload(&ctl->stop) || now - idle_since > idle_ns) {
+                const long long last = vload(&ctl->last_claim_ns);
+                const long long ref = last > t_start ? last : t_start;
+                if (vload(&ctl->exiting) || vload(&ctl->stop) || now - ref > idle_ns) {
+                    atomicExch(&ctl->exiting, 1);
                     slot = -2;
                 } else {
                     __nanosleep(backoff);
@@ -387,9 +394,10 @@ void ensure_loop(ksim_server *s)
     for (ServeRequest *r : s->running)
         if (r->loop && r->state == R_RUNNING) need = true;
     if (!need) return;
-    // start after everything published so far has landed
+    // start after everything published so far has landed, with the exit word clear
     cudaError_t e = cudaEventRecord(s->h2d_mark, s->s_h2d);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s->s_loop, s->h2d_mark, 0);
+    if (e == cudaSuccess) e = cudaMemsetAsync(&s->d_ctl->exiting, 0, sizeof(int32_t), s->s_loop);
     if (e == cudaSuccess) {
         k_serve<<<s->grid, s->lcfg.threads, s->smem, s->s_loop>>>(s->d_jobs, s->d_reqs, s->d_ring, s->ring_cap,
                                                                    s->d_ctl, s->d_done,
@@ -548,9 +556,9 @@ ksim_status ksim_server_create(const ksim_server_config *cfg_in, ksim_server **o
     if (cfg.arena_bytes <= 0) cfg.arena_bytes = (int64_t)1 << 30;
     if (cfg.max_requests <= 0) cfg.max_requests = 1024;
     if (cfg.max_jobs <= 0) cfg.max_jobs = 4096;
-    if (cfg.threads <= 0) cfg.threads = 256;
+    if (cfg.threads <= 0) cfg.threads = 128;
     if (cfg.slot_bytes <= 0) cfg.slot_bytes = 16384;
-    if (cfg.idle_us <= 0) cfg.idle_us = 1000;
+    if (cfg.idle_us <= 0) cfg.idle_us = 2000;
     if (cfg.threads > 256 || (cfg.threads & 31))
         return fail(KSIM_ERR_INVALID_ARGUMENT, "threads must be a multiple of 32 in [32, 256]");
     if ((cfg.slot_bytes & 15) || staged_smem_bytes(cfg.slot_bytes) > 227 * 1024)
