@@ -20,6 +20,14 @@ JSON line on rank 0.
   this GPU by ksim_measure_int_peak.
 * ``cpu_baseline``: the reference's own zx_eval.hpp (oracle/_ref) or its C
   restatement, all host threads, on a bounded shot sample.
+* ``batched`` (1 GPU): 64 seeded programs (qubits U[8,60], t U[2,16], shots
+  log-uniform 1e3-1e5) in one persistent graph-replayed launch, autotuned,
+  vs 64 plain one-program launches; device time, L2 flushed, bit identity
+  of the two checked.
+* ``served`` (1 GPU): 10 000 Poisson requests over a 200-program pool at
+  80 % of the measured served capacity through the continuous-batching
+  server: shots/s and p50/p99 latency (arrival -> bits in host memory, host
+  clock), vs the same stream through plain per-request calls.
 
 ``--impl reference`` times that CPU implementation alone on the same workload
 (rank 0 only under torchrun).
@@ -57,6 +65,11 @@ def parse():
     ap.add_argument("--rng", type=int, default=0, help="0 xorshift (kokkos_sim), 1 philox")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched (64-program) leg")
+    ap.add_argument("--no-served", action="store_true", help="skip the served (request stream) leg")
+    ap.add_argument("--requests", type=int, default=10_000, help="requests of the served leg")
+    ap.add_argument("--load", type=float, default=0.8,
+                    help="served arrival rate as a fraction of the measured served capacity")
     return ap.parse_args()
 
 
@@ -213,6 +226,193 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def _timed_launches(torch, stream, flush, fn, steps):
+    """Device ms of `steps` calls of fn(i), L2 flushed before each (CUDA events)."""
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(steps)]
+    for i in range(steps):
+        flush.zero_()
+        evs[i][0].record(stream)
+        fn(i)
+        evs[i][1].record(stream)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in evs]
+
+
+def bench_batched(args, torch, dev, flush):
+    """Workload 3: 64 programs in one persistent graph-captured launch vs 64
+    plain one-program launches on the same GPU, same inputs."""
+    from ksim_b200 import synth
+    from ksim_b200.batch import BatchSampler
+    ws = synth.batched_workloads()
+    rng = np.random.default_rng(3001)
+    fs = [synth.sample_f(rng, w.shots, w.n_f, w.f_prob) for w in ws]
+    seeds = [w.seed for w in ws]
+    bs = BatchSampler([w.program for w in ws], [w.shots for w in ws], seeds=seeds,
+                      rng_mode=args.rng, device=dev.index or 0, n_f=[w.n_f for w in ws])
+    bs.set_inputs(fs)
+    rec = bs.tune()
+    stream = torch.cuda.current_stream(dev)
+    bs.launch_plain(stream)
+    plain_bits = bs.results()
+    bs.launch(stream)
+    same = all(np.array_equal(a, b) for a, b in zip(bs.results(), plain_bits))
+    for _ in range(max(3, args.warmup)):
+        bs.launch(stream)
+        bs.launch_plain(stream)
+    steps = max(3, args.steps)
+    t_batch = _timed_launches(torch, stream, flush, lambda i: bs.launch(stream), steps)
+    t_plain = _timed_launches(torch, stream, flush, lambda i: bs.launch_plain(stream), steps)
+    total = bs.total_shots
+    mb, mp = sum(t_batch) / steps, sum(t_plain) / steps
+    info = bs.info()
+    return {"workload": f"cfg3-batched: {len(ws)} programs, qubits U[8,60], t U[2,16], "
+                        f"shots log-U[1e3,1e5] ({total} shots)",
+            "shots_per_s": total / (mb / 1e3), "ms_per_batch": mb,
+            "plain_shots_per_s": total / (mp / 1e3), "plain_ms": mp,
+            "speedup_vs_plain": mp / mb, "bit_identical_to_plain": bool(same),
+            "launch": "1 persistent kernel in a CUDA graph" if info["launches"] == 1
+                      else f"{info['launches']} persistent kernels in a CUDA graph",
+            "plain_launches": len(ws), "tuning": rec["tuning"], "work_items": info["items"],
+            "grid": info["grid"]}
+
+
+class _PinnedRing:
+    """FIFO allocator of output rows in one page-locked buffer (requests are
+    retired in submission order)."""
+
+    def __init__(self, torch, nbytes):
+        self.buf = torch.empty(nbytes, dtype=torch.uint8).pin_memory().numpy()
+        self.n = nbytes
+        self.head = self.tail = 0      # byte counters (mod n)
+        self.live = []                 # (start, end) in submission order
+        self.cv = threading.Condition()
+
+    def alloc(self, nbytes):
+        nbytes = max(nbytes, 1)
+        with self.cv:
+            while True:
+                pos = self.head % self.n
+                skip = self.n - pos if pos + nbytes > self.n else 0   # no block across the wrap
+                if self.head + skip + nbytes - self.tail <= self.n:
+                    start = self.head + skip
+                    self.head = start + nbytes
+                    self.live.append((start, self.head))
+                    s = start % self.n
+                    return self.buf[s:s + nbytes]
+                self.cv.wait()
+
+    def free_oldest(self):
+        with self.cv:
+            self.live.pop(0)
+            self.tail = self.live[0][0] if self.live else self.head
+            self.cv.notify_all()
+
+
+def _replay(arrivals, submit, collect):
+    """Submit request i at arrivals[i] (seconds from start) on one thread and
+    collect results in order on another; returns (start, done times)."""
+    import queue
+    q = queue.Queue()
+    done = [0.0] * len(arrivals)
+    t0 = time.perf_counter() + 0.05
+
+    def producer():
+        for i, a in enumerate(arrivals):
+            dt = t0 + a - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            q.put((i, submit(i)))
+        q.put(None)
+
+    def consumer():
+        while True:
+            item = q.get()
+            if item is None:
+                return
+            i, h = item
+            done[i] = collect(i, h)
+
+    th = [threading.Thread(target=producer), threading.Thread(target=consumer)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    return t0, done
+
+
+def bench_served(args, torch, dev):
+    """Workload 5: a Poisson stream of sample requests over a 200-program pool
+    through the continuous-batching server, and the same stream through plain
+    per-request calls (B200ProgramSampler.sample) on the same GPU."""
+    from ksim_b200 import synth
+    from ksim_b200.sampler import B200ProgramSampler
+    from ksim_b200.serve import Server
+    pool = synth.serving_pool()
+    rng = np.random.default_rng(5555)
+    n_req = args.requests
+    pidx = rng.integers(0, len(pool), n_req)
+    shots = np.round(np.exp(rng.uniform(np.log(1e2), np.log(1e5), n_req))).astype(np.int64)
+    rows = 100_000
+    wide = torch.from_numpy(synth.sample_f(rng, rows, 128, 0.02)).pin_memory().numpy()
+    r0 = (rng.random(n_req) * (rows - shots + 1)).astype(np.int64)
+    seeds = rng.integers(0, 2**62, n_req)
+    n_out = [p.program.num_outputs for p in pool]
+    ring = _PinnedRing(torch, 1 << 30)
+
+    srv = Server(device=dev.index or 0, arena_bytes=4 << 30)
+    for w in pool:                       # programs resident on the device before the stream
+        d, _ = srv.cache.acquire(w.program)
+        srv.cache.release(d)
+
+    def submit(i):
+        B = int(shots[i])
+        out = ring.alloc(B * n_out[pidx[i]]).reshape(B, n_out[pidx[i]])
+        return srv.submit(pool[pidx[i]].program, wide[r0[i]:r0[i] + B], int(seeds[i]),
+                          args.rng, out=out)
+
+    def collect(i, h):
+        h.result()
+        ring.free_oldest()
+        return h.done_time_s
+
+    # capacity: a closed burst of the first requests, all submitted at once
+    n_probe = min(n_req, 1500)
+    t0, done = _replay([0.0] * n_probe, submit, collect)
+    capacity = float(shots[:n_probe].sum()) / (max(done) - t0)
+    rate = args.load * capacity / float(shots.mean())
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+    before = srv.stats()
+    t0, done = _replay(arrivals, submit, collect)
+    lat = np.array(done) - (t0 + arrivals)
+    served = float(shots.sum()) / (max(done) - t0)
+    st = srv.stats()
+    srv.close()
+
+    # the same stream through plain per-request calls, in arrival order
+    samplers = {k: B200ProgramSampler(pool[k].program, device=dev.index or 0)
+                for k in set(int(x) for x in pidx)}   # uploads outside the timed stream
+
+    def pcollect(i, _):
+        B = int(shots[i])
+        samplers[int(pidx[i])].sample(wide[r0[i]:r0[i] + B], int(seeds[i]), rng_mode=args.rng)
+        return time.perf_counter()
+
+    pt0, pdone = _replay(arrivals, lambda i: i, pcollect)
+    plat = np.array(pdone) - (pt0 + arrivals)
+    plain = float(shots.sum()) / (max(pdone) - pt0)
+    q = lambda a, x: float(np.percentile(a, x) * 1e3)  # noqa: E731
+    return {"workload": f"cfg5-served: {n_req} Poisson requests over {len(pool)} programs "
+                        f"(cfg2/3/4 generators), shots log-U[1e2,1e5], f rows 128 B",
+            "shots_per_s": served, "p50_ms": q(lat, 50), "p99_ms": q(lat, 99),
+            "plain_shots_per_s": plain, "plain_p50_ms": q(plat, 50), "plain_p99_ms": q(plat, 99),
+            "speedup_vs_plain": served / plain,
+            "arrival_rate_per_s": rate, "load": args.load, "capacity_shots_per_s": capacity,
+            "total_shots": int(shots.sum()),
+            "loop_launches": st["loop_launches"] - before["loop_launches"],
+            "failed": st["failed"], "clock": "host wall clock, arrival -> results in host memory"}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -288,6 +488,12 @@ def main():
         cpu = {"value": rate, "unit": "shots/s", "cores": cores, "kind": kind,
                "sample": f"first {n} shots of {w.name}, {dt:.1f} s on {cores} threads"}
 
+    batched = served = None
+    if world == 1 and not args.no_batched:
+        batched = bench_batched(args, torch, dev, flush)
+    if world == 1 and not args.no_served:
+        served = bench_served(args, torch, dev)
+
     if rank == 0:
         mean_s = (sum(step_ms) / len(step_ms)) / 1e3
         achieved = work["ops"] * shots / mean_s
@@ -311,6 +517,8 @@ def main():
                          "ops_per_shot": work["ops"], "hbm_gbs": hbm_bytes / mean_s / 1e9,
                          "peak_source": "ksim_measure_int_peak on this GPU (burst)"},
             "cpu_baseline": cpu,
+            "batched": batched,
+            "served": served,
             "clocks": clk.summary(),
             "gpu_launches": args.steps * len(prog.components),
             "step_ms": step_ms,
