@@ -74,31 +74,43 @@ def parse():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks / throttle reasons every 20 ms; summary() keeps the
+    samples taken inside the timed region (between begin() and end())."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, period_ms: int = 20):
         self.index = index
+        self.period_ms = period_ms
         self.proc = None
-        self.lines = []
+        self.lines = []  # (perf_counter, line)
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", str(self.period_ms)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            deadline = time.perf_counter() + 3.0   # the first sample takes a moment
+            while not self.lines and time.perf_counter() < deadline:
+                time.sleep(0.01)
         except (FileNotFoundError, OSError):
             self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
+
+    def begin(self):
+        self.t0 = time.perf_counter()
+
+    def end(self):
+        self.t1 = time.perf_counter()
 
     def __exit__(self, *exc):
         if self.proc:
@@ -111,7 +123,11 @@ class ClockSampler:
     def summary(self) -> dict:
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        t0 = self.t0 if self.t0 is not None else float("-inf")
+        t1 = self.t1 if self.t1 is not None else float("inf")
+        for ts, ln in self.lines:
+            if not t0 <= ts <= t1 + self.period_ms / 1e3:
+                continue
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -124,7 +140,8 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "period_ms": self.period_ms}
 
 
 def dist_setup(args):
@@ -455,12 +472,14 @@ def main():
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
            for _ in range(args.steps)]
     with ClockSampler(local) as clk:
+        clk.begin()
         for i in range(args.steps):
             flush.zero_()
             evs[i][0].record(stream)
             launch(2000 + i)
             evs[i][1].record(stream)
         torch.cuda.synchronize()
+        clk.end()
     barrier(world)
     torch.cuda.synchronize()
     step_ms = [a.elapsed_time(b) for a, b in evs]

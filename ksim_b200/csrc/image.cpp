@@ -325,7 +325,9 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 err = gname + ": a term has more than 65535 columns in one family";
                 return KSIM_ERR_UNSUPPORTED;
             }
-            uint32_t flags = unsafe ? TF_SLOW : 0u;
+            // every value the fast path must know exactly is below 2^Lmax; with
+            // Lmax <= 30.5 it fits int32 and the term runs on 32-bit words
+            uint32_t flags = unsafe ? TF_SLOW : (Lmax <= 30.5 ? TF_NARROW : 0u);
             if (g.pf_has_approx) flags |= TF_APX;
             put32(out, (uint32_t)n_np | ((uint32_t)n_hp << 16));
             put32(out, (uint32_t)n_pp | ((uint32_t)n_ph << 16));
@@ -346,6 +348,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             img.max_term_bytes = std::max(img.max_term_bytes, tb);
             img.n_terms += 1;
             img.n_slow_terms += unsafe ? 1 : 0;
+            img.n_narrow_terms += (flags & TF_NARROW) ? 1 : 0;
             img.n_columns += n_np + n_hp + n_pp + n_ph;
         }
         toff.push_back((int64_t)out.size());

@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(128) k_eval(const EvalJob j)
         for (int t = 0; t < gd.G; ++t) {
             const TermHdr h = load_hdr(p);
             TermOut r;
-            p = (h.flags & TF_SLOW) ? eval_term_exact<W>(p, h, v, r) : eval_term_fast<W>(p, h, v, r);
+            p = eval_term<W>(p, h, v, r);
             o[5 * t + 0] = (int64_t)r.z.a;
             o[5 * t + 1] = (int64_t)r.z.b;
             o[5 * t + 2] = (int64_t)r.z.c;

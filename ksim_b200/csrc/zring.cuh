@@ -40,7 +40,10 @@
 namespace ksim {
 
 // ---- image record layout (shared with image.cpp) --------------------------
-enum : uint32_t { TF_SLOW = 1u, TF_APX = 2u };
+// TF_SLOW: evaluate step by step (no proof the fast path stays in range);
+// TF_NARROW: every value the fast path must know exactly (at each halving
+// and at the end) is proven below 2^31, so it runs on 32-bit coefficients.
+enum : uint32_t { TF_SLOW = 1u, TF_APX = 2u, TF_NARROW = 4u };
 constexpr int TERM_HDR_BYTES = 32;
 constexpr int TERM_APX_BYTES = 16;
 // NodePhases / HalfPi column: W mask words + 1 constant word, padded to 16 B
@@ -50,9 +53,24 @@ KS_HD constexpr int rec2_words(int W) { return (2 * W + 2) & ~1; }
 constexpr uint32_t NP_REDUCE_BIT = 8u;
 constexpr uint32_t NU_ZERO = 15u;  // PhasePairs factor is exactly zero
 
-struct Zu { uint64_t a, b, c, d; };
+// Coefficients as unsigned words, so every add and multiply wraps like the
+// reference's int64 (T = uint64_t) or, on the narrow path, like int32.
+template <typename T>
+struct Zr { T a, b, c, d; };
+using Zu = Zr<uint64_t>;
+using Zn = Zr<uint32_t>;
 
-KS_HD uint64_t sneg(uint64_t x, uint64_t m) { return (x ^ m) - m; }  // m = 0: x, m = ~0: -x
+template <typename T>
+KS_HD T sneg(T x, T m) { return (x ^ m) - m; }  // m = 0: x, m = ~0: -x
+
+// acc + (m ? -x : x).  64-bit: xor/subtract on the integer ALU; 32-bit: one
+// multiply-add by +-1, which runs on the FMA pipe and leaves the ALU free.
+KS_HD uint64_t cadd(uint64_t acc, uint64_t x, uint64_t m) { return acc + sneg(x, m); }
+KS_HD uint32_t cadd(uint32_t acc, uint32_t x, uint32_t m) { return acc + (m | 1u) * x; }
+
+// Arithmetic shift right of the signed value held in x.
+KS_HD uint64_t sshr(uint64_t x, uint32_t n) { return (uint64_t)((int64_t)x >> n); }
+KS_HD uint32_t sshr(uint32_t x, uint32_t n) { return (uint32_t)((int32_t)x >> n); }
 
 KS_HD uint32_t popc64(uint64_t x)
 {
@@ -119,39 +137,43 @@ KS_HD double pow2i(int64_t n)
 }
 
 // z * w^k for a per-shot k in 0..7 (selects, no branches).
-KS_HD Zu rot_var(Zu z, uint32_t k)
+template <typename T>
+KS_HD Zr<T> rot_var(Zr<T> z, uint32_t k)
 {
     const bool k1 = k & 1u, k2 = k & 2u;
-    Zu r;
+    Zr<T> r;
     r.a = k1 ? z.d : z.a;
     r.b = k1 ? z.a : z.b;
     r.c = k1 ? z.b : z.c;
-    r.d = k1 ? (0 - z.c) : z.d;
-    Zu q;
-    q.a = k2 ? (0 - r.c) : r.a;
+    r.d = k1 ? (T)(0 - z.c) : z.d;
+    Zr<T> q;
+    q.a = k2 ? (T)(0 - r.c) : r.a;
     q.b = k2 ? r.d : r.b;
     q.c = k2 ? r.a : r.c;
-    q.d = k2 ? (0 - r.b) : r.d;
-    const uint64_t m = 0 - (uint64_t)((k >> 2) & 1u);
+    q.d = k2 ? (T)(0 - r.b) : r.d;
+    const T m = (T)0 - (T)((k >> 2) & 1u);
     q.a = sneg(q.a, m); q.b = sneg(q.b, m); q.c = sneg(q.c, m); q.d = sneg(q.d, m);
     return q;
 }
 
 // acc += s * R_j(t), s = +1 (m = 0) or -1 (m = ~0), j in 0..3 the same for all shots.
-KS_HD void add_rot(Zu &acc, const Zu &t, uint32_t j, uint64_t m)
+template <typename T>
+KS_HD void add_rot(Zr<T> &acc, const Zr<T> &t, uint32_t j, T m)
 {
+    const T n = ~m;  // the opposite sign
     switch (j & 3u) {
-    case 0: acc.a += sneg(t.a, m); acc.b += sneg(t.b, m); acc.c += sneg(t.c, m); acc.d += sneg(t.d, m); break;
-    case 1: acc.a += sneg(t.d, m); acc.b += sneg(t.a, m); acc.c += sneg(t.b, m); acc.d -= sneg(t.c, m); break;
-    case 2: acc.a -= sneg(t.c, m); acc.b += sneg(t.d, m); acc.c += sneg(t.a, m); acc.d -= sneg(t.b, m); break;
-    default: acc.a -= sneg(t.b, m); acc.b -= sneg(t.c, m); acc.c += sneg(t.d, m); acc.d -= sneg(t.a, m); break;
+    case 0: acc.a = cadd(acc.a, t.a, m); acc.b = cadd(acc.b, t.b, m); acc.c = cadd(acc.c, t.c, m); acc.d = cadd(acc.d, t.d, m); break;
+    case 1: acc.a = cadd(acc.a, t.d, m); acc.b = cadd(acc.b, t.a, m); acc.c = cadd(acc.c, t.b, m); acc.d = cadd(acc.d, t.c, n); break;
+    case 2: acc.a = cadd(acc.a, t.c, n); acc.b = cadd(acc.b, t.d, m); acc.c = cadd(acc.c, t.a, m); acc.d = cadd(acc.d, t.b, n); break;
+    default: acc.a = cadd(acc.a, t.b, n); acc.b = cadd(acc.b, t.c, n); acc.c = cadd(acc.c, t.d, m); acc.d = cadd(acc.d, t.a, n); break;
     }
 }
 
 // Full product (zx_eval.hpp:27-33 formula, basis (1, w, i, conj w)).
-KS_HD Zu zmul(const Zu &x, const Zu &y)
+template <typename T>
+KS_HD Zr<T> zmul(const Zr<T> &x, const Zr<T> &y)
 {
-    Zu r;
+    Zr<T> r;
     r.a = x.a * y.a + x.b * y.d - x.c * y.c + x.d * y.b;
     r.b = x.a * y.b + x.b * y.a + x.c * y.d + x.d * y.c;
     r.c = x.a * y.c + x.b * y.b + x.c * y.a - x.d * y.d;
@@ -159,22 +181,34 @@ KS_HD Zu zmul(const Zu &x, const Zu &y)
     return r;
 }
 
-KS_HD void shr1_all(Zu &z)
+template <typename T>
+KS_HD void shr_all(Zr<T> &z, uint32_t n)
 {
-    z.a = (uint64_t)((int64_t)z.a >> 1);
-    z.b = (uint64_t)((int64_t)z.b >> 1);
-    z.c = (uint64_t)((int64_t)z.c >> 1);
-    z.d = (uint64_t)((int64_t)z.d >> 1);
+    z.a = sshr(z.a, n); z.b = sshr(z.b, n); z.c = sshr(z.c, n); z.d = sshr(z.d, n);
 }
 
+KS_HD void shr1_all(Zu &z) { shr_all(z, 1u); }
+
 // One renormalisation step with the explicit test (zx_eval.hpp:35-41).
-KS_HD void zreduce(Zu &z, int64_t &pw)
+template <typename T>
+KS_HD void zreduce(Zr<T> &z, int64_t &pw)
 {
-    const uint64_t o = z.a | z.b | z.c | z.d;
+    const T o = z.a | z.b | z.c | z.d;
     if (o != 0 && (o & 1u) == 0) {
-        shr1_all(z);
+        shr_all(z, 1u);
         pw += 1;
     }
+}
+
+// Sign-extend a narrow element to the 64-bit representation.
+KS_HD Zu widen(const Zn &z)
+{
+    Zu r;
+    r.a = (uint64_t)(int64_t)(int32_t)z.a;
+    r.b = (uint64_t)(int64_t)(int32_t)z.b;
+    r.c = (uint64_t)(int64_t)(int32_t)z.c;
+    r.d = (uint64_t)(int64_t)(int32_t)z.d;
+    return r;
 }
 
 KS_HD bool over62(const Zu &z)
@@ -235,14 +269,18 @@ struct TermOut {
     uint32_t risk;  // KSIM_FLAG_INT64_RISK raised by the exact path
 };
 
-// Fast path: exact when the host proved every coefficient stays below 2^62.
-template <int W>
+// Fast path: exact when the host proved every coefficient stays below 2^62
+// (T = uint64_t) or that every value it must know exactly stays below 2^31
+// (T = uint32_t, TF_NARROW): adds and multiplies wrap, so intermediate sums
+// may leave the narrow range, but the values at each halving and at the end
+// are the true ones.
+template <int W, typename T = uint64_t>
 KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const uint64_t (&v)[W],
                                     TermOut &o)
 {
     constexpr int R1 = rec1_words(W), R2 = rec2_words(W);
     const uint64_t *q = (const uint64_t *)(p + TERM_HDR_BYTES + ((h.flags & TF_APX) ? TERM_APX_BYTES : 0));
-    Zu z = {1, 0, 0, 0};
+    Zr<T> z = {1, 0, 0, 0};
     int64_t pw = 0;
     uint32_t alive = 1;
 
@@ -260,13 +298,13 @@ KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const ui
             // factor 2 (halved straight back, pw + 1) or 0 (the term dies)
             pw += alive & (neg ^ 1u);
             alive &= neg ^ 1u;
-            const uint64_t keep = 0 - (uint64_t)alive;
+            const T keep = (T)0 - (T)alive;
             z.a &= keep; z.b &= keep; z.c &= keep; z.d &= keep;
         } else {
-            const Zu t0 = z;
-            add_rot(z, t0, j, 0 - (uint64_t)neg);
+            const Zr<T> t0 = z;
+            add_rot(z, t0, j, (T)0 - (T)neg);
             if (cw & NP_REDUCE_BIT) {
-                shr1_all(z);
+                shr_all(z, 1u);
                 pw += alive;
             }
         }
@@ -298,7 +336,7 @@ KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const ui
             const uint32_t phi = ((cw >> 1) ^ parity<W>(mb, v)) & 1u;
             e ^= psi & phi;
         }
-        const uint64_t m = 0 - (uint64_t)e;
+        const T m = (T)0 - (T)e;
         z.a = sneg(z.a, m); z.b = sneg(z.b, m); z.c = sneg(z.c, m); z.d = sneg(z.d, m);
     }
     // PhasePairs: per-shot valuation tracking
@@ -313,27 +351,29 @@ KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const ui
             const uint32_t cw = (uint32_t)r[2 * W];
             const uint32_t pa = parity<W>(ma, v), pb = parity<W>(mb, v);
             const uint32_t ac = cw & 7u, bc = (cw >> 3) & 7u, gc = (ac + bc) & 7u;
-            const Zu t0 = z;
-            add_rot(z, t0, ac & 3u, 0 - (uint64_t)(((ac >> 2) ^ pa) & 1u));
-            add_rot(z, t0, bc & 3u, 0 - (uint64_t)(((bc >> 2) ^ pb) & 1u));
-            add_rot(z, t0, gc & 3u, 0 - (uint64_t)(((gc >> 2) ^ pa ^ pb ^ 1u) & 1u));
+            const Zr<T> t0 = z;
+            add_rot(z, t0, ac & 3u, (T)0 - (T)(((ac >> 2) ^ pa) & 1u));
+            add_rot(z, t0, bc & 3u, (T)0 - (T)(((bc >> 2) ^ pb) & 1u));
+            add_rot(z, t0, gc & 3u, (T)0 - (T)(((gc >> 2) ^ pa ^ pb ^ 1u) & 1u));
             const uint32_t nf = (cw >> (8 + 4 * (pa | (pb << 1)))) & 15u;
             alive &= (nf != NU_ZERO) ? 1u : 0u;
             nu += nf;
             const uint32_t red = alive & (nu >= 4 ? 1u : 0u);
             nu -= 4 * red;
-            z.a = (uint64_t)((int64_t)z.a >> red);
-            z.b = (uint64_t)((int64_t)z.b >> red);
-            z.c = (uint64_t)((int64_t)z.c >> red);
-            z.d = (uint64_t)((int64_t)z.d >> red);
+            shr_all(z, red);
             pw += red;
         }
     }
     // prefactor: w^idx, then the exact floatfactor with one renormalisation
     z = rot_var(z, h.pf_idx);
-    z = zmul(z, h.ff);
+    const Zr<T> ff = {(T)h.ff.a, (T)h.ff.b, (T)h.ff.c, (T)h.ff.d};
+    z = zmul(z, ff);
     zreduce(z, pw);
-    o.z = z;
+    if constexpr (sizeof(T) == 8) {
+        o.z = z;
+    } else {
+        o.z = widen(z);
+    }
     o.pw = pw;
     o.power2 = h.power2;
     o.risk = 0;
@@ -422,6 +462,15 @@ KS_HD void term_complex(const TermOut &o, const uint8_t *hdr_ptr, uint32_t flags
     }
 }
 
+// One term on the path its header selects.  Returns the next record.
+template <int W>
+KS_HD const uint8_t *eval_term(const uint8_t *p, const TermHdr &h, const uint64_t (&v)[W], TermOut &o)
+{
+    if (h.flags & TF_SLOW) return eval_term_exact<W>(p, h, v, o);
+    if (h.flags & TF_NARROW) return eval_term_fast<W, uint32_t>(p, h, v, o);
+    return eval_term_fast<W, uint64_t>(p, h, v, o);
+}
+
 // Evaluate `n_terms` consecutive term records starting at p, adding their
 // complex values to (sum_re, sum_im) in order.  Returns the end pointer.
 template <int W>
@@ -431,8 +480,7 @@ KS_HD const uint8_t *eval_terms(const uint8_t *p, uint32_t n_terms, const uint64
     for (uint32_t t = 0; t < n_terms; ++t) {
         const TermHdr h = load_hdr(p);
         TermOut o;
-        const uint8_t *next = (h.flags & TF_SLOW) ? eval_term_exact<W>(p, h, v, o)
-                                                  : eval_term_fast<W>(p, h, v, o);
+        const uint8_t *next = eval_term<W>(p, h, v, o);
         double re, im;
         term_complex(o, p, h.flags, re, im);
         sum_re = dadd(sum_re, re);

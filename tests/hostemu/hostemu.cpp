@@ -42,7 +42,7 @@ void eval_rows(const HostImage &img, int gi, const uint8_t *params, int64_t B, i
             for (int t = 0; t < gd.G; ++t) {
                 const TermHdr h = load_hdr(p);
                 TermOut r;
-                p = (h.flags & TF_SLOW) ? eval_term_exact<W>(p, h, v, r) : eval_term_fast<W>(p, h, v, r);
+                p = eval_term<W>(p, h, v, r);
                 o[5 * t] = (int64_t)r.z.a;
                 o[5 * t + 1] = (int64_t)r.z.b;
                 o[5 * t + 2] = (int64_t)r.z.c;
