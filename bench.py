@@ -52,6 +52,11 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = ("shots/sec at 1 B200, batched+served vs plain, bit-exact Z[ω]; p50/p99 latency")
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes per shot of the plain kernel, from one ncu capture of
+# k_sample on the same workload at 262,144 shots (dram__bytes_read.sum +
+# dram__bytes_write.sum), plus the output row the capture's L2 absorbed;
+# scaled to a launch by its shots.  Source: profiles/k_sample_cfg2_narrow.md.
+NCU_DRAM_BYTES_PER_SHOT = {"cfg2-medium-40q-t12": 66.5 + 40.0}
 
 
 def parse():
@@ -532,7 +537,10 @@ def main():
                     "d2h_bytes_per_step": int(shots * n_out)},
             "roofline": {"bound": "alu", "achieved": achieved / 1e9, "peak": peak.value / 1e9,
                          "unit": "Gop/s (int32)", "frac": achieved / peak.value,
-                         "traffic": None,
+                         "traffic": (NCU_DRAM_BYTES_PER_SHOT[w.name] * shots
+                                     if w.name in NCU_DRAM_BYTES_PER_SHOT else None),
+                         "traffic_unit": "bytes per launch",
+                         "algorithmic_bytes": hbm_bytes,
                          "ops_per_shot": work["ops"], "hbm_gbs": hbm_bytes / mean_s / 1e9,
                          "peak_source": "ksim_measure_int_peak on this GPU (burst)"},
             "cpu_baseline": cpu,

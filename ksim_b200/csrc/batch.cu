@@ -41,7 +41,7 @@ struct BatchItem {
 namespace {
 
 template <int CLASS>
-__global__ void __launch_bounds__(256) k_batch(const BatchJobDev *__restrict__ jobs,
+__global__ void __launch_bounds__(256, CLASS == 0 ? KSIM_SAMPLE_MIN_CTAS : 1) k_batch(const BatchJobDev *__restrict__ jobs,
                                                const BatchItem *__restrict__ items, int n_items, int *counter)
 {
     extern __shared__ __align__(128) uint8_t smem[];
@@ -61,19 +61,19 @@ __global__ void __launch_bounds__(256) k_batch(const BatchJobDev *__restrict__ j
         bool ok = true;
         if (CLASS == 0) {
             switch (J.W) {
-            case 1: ok = sample_tile<1, true>(J.j, w.s0, bar, slots, g); break;
-            case 2: ok = sample_tile<2, true>(J.j, w.s0, bar, slots, g); break;
-            case 3: ok = sample_tile<3, true>(J.j, w.s0, bar, slots, g); break;
-            default: ok = sample_tile<4, true>(J.j, w.s0, bar, slots, g); break;
+            case 1: ok = sample_tile<1, true, false, shots_per_thread(1)>(J.j, w.s0, bar, slots, g); break;
+            case 2: ok = sample_tile<2, true, false, shots_per_thread(2)>(J.j, w.s0, bar, slots, g); break;
+            case 3: ok = sample_tile<3, true, false, shots_per_thread(3)>(J.j, w.s0, bar, slots, g); break;
+            default: ok = sample_tile<4, true, false, shots_per_thread(4)>(J.j, w.s0, bar, slots, g); break;
             }
         } else {
             switch (J.W) {
-            case 5: ok = sample_tile<5, true>(J.j, w.s0, bar, slots, g); break;
-            case 6: ok = sample_tile<6, true>(J.j, w.s0, bar, slots, g); break;
-            case 8: ok = sample_tile<8, true>(J.j, w.s0, bar, slots, g); break;
-            case 10: ok = sample_tile<10, true>(J.j, w.s0, bar, slots, g); break;
-            case 12: ok = sample_tile<12, true>(J.j, w.s0, bar, slots, g); break;
-            default: ok = sample_tile<16, true>(J.j, w.s0, bar, slots, g); break;
+            case 5: ok = sample_tile<5, true, false, shots_per_thread(5)>(J.j, w.s0, bar, slots, g); break;
+            case 6: ok = sample_tile<6, true, false, shots_per_thread(6)>(J.j, w.s0, bar, slots, g); break;
+            case 8: ok = sample_tile<8, true, false, shots_per_thread(8)>(J.j, w.s0, bar, slots, g); break;
+            case 10: ok = sample_tile<10, true, false, shots_per_thread(10)>(J.j, w.s0, bar, slots, g); break;
+            case 12: ok = sample_tile<12, true, false, shots_per_thread(12)>(J.j, w.s0, bar, slots, g); break;
+            default: ok = sample_tile<16, true, false, shots_per_thread(16)>(J.j, w.s0, bar, slots, g); break;
             }
         }
         if (!ok) break;
@@ -192,12 +192,13 @@ ksim_status ksim_batch_create(const ksim_batch_job *jobs, int32_t n_jobs, const 
         double bytes = 0;
         for (const GraphDir &gd : c->img.gdir) bytes += (double)gd.stream_bytes + 64.0;
         const int cls = d.W <= 4 ? 0 : 1;
-        for (int64_t s0 = 0; s0 < jb.B; s0 += b->threads) {
+        const int64_t tile = (int64_t)b->threads * shots_per_thread(d.W);
+        for (int64_t s0 = 0; s0 < jb.B; s0 += tile) {
             BatchItem it = {};
             it.job = i;
             it.s0 = s0;
             items[cls].push_back(it);
-            cost[cls].push_back(bytes * (double)std::min<int64_t>(b->threads, jb.B - s0));
+            cost[cls].push_back(bytes * (double)std::min<int64_t>(tile, jb.B - s0));
         }
     }
     cudaError_t e = cudaMalloc(&b->d_jobs, sizeof(BatchJobDev) * b->host_jobs.size());

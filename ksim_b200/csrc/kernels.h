@@ -5,7 +5,22 @@
 
 #include "image.h"
 
+// Resident CTAs of 256 threads per SM the sampling kernels are compiled for
+// (it caps registers at 65536 / (256 * n)); the W > 4 batch kernel uses 1.
+#ifndef KSIM_SAMPLE_MIN_CTAS
+#define KSIM_SAMPLE_MIN_CTAS 2
+#endif
+
+// Shots one thread of the sampling kernels carries for parameter vectors of
+// W words: two for W <= 4 (each column record is decoded once for both, and
+// the two shots are independent dependency chains), one for wider vectors.
+#ifndef KSIM_SHOTS_PER_THREAD
+#define KSIM_SHOTS_PER_THREAD 2
+#endif
+
 namespace ksim {
+
+__host__ __device__ constexpr int shots_per_thread(int W) { return W <= 4 ? KSIM_SHOTS_PER_THREAD : 1; }
 
 // One sampling job: a component image, its input rows and output placement.
 struct SampleJob {

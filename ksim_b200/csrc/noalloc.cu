@@ -50,14 +50,15 @@ std::mutex g_scratch_mu;
 uint8_t *g_scratch_addr[NOALLOC_MAX_DEVICES] = {};
 
 template <int W, bool STAGED>
-__global__ void __launch_bounds__(256) k_sample_noalloc(const SampleJob j)
+__global__ void __launch_bounds__(256, KSIM_SAMPLE_MIN_CTAS) k_sample_noalloc(const SampleJob j)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     uint64_t *bar = (uint64_t *)smem;
     uint8_t *slots = smem + BAR_BYTES;
     if (STAGED) ring_init(bar);
     uint32_t g = 0;
-    sample_tile<W, STAGED>(j, (int64_t)blockIdx.x * blockDim.x, bar, slots, g);
+    constexpr int S = shots_per_thread(W);
+    sample_tile<W, STAGED, false, S>(j, (int64_t)blockIdx.x * blockDim.x * S, bar, slots, g);
 }
 
 // Set-up, once per device, with that device current.
@@ -116,7 +117,8 @@ int chunks_into(const HostImage &img, int64_t slot_bytes, ChunkDir *out, int cap
 template <int W>
 cudaError_t launch_noalloc_w(const SampleJob &j, const LaunchCfg &cfg, cudaStream_t st)
 {
-    const int64_t blocks = (j.B + cfg.threads - 1) / cfg.threads;
+    const int64_t tile = (int64_t)cfg.threads * shots_per_thread(W);
+    const int64_t blocks = (j.B + tile - 1) / tile;
     if (blocks > 0x7FFFFFFF) return cudaErrorInvalidConfiguration;
     if (cfg.staged) {
         const size_t smem = staged_smem_bytes(j.slot_bytes);

@@ -169,37 +169,56 @@ __device__ __forceinline__ void issue_chunk(const SampleJob &j, int c, uint32_t 
 // Sample shots [s0, s0 + blockDim.x) of job j.  g is the CTA's running chunk
 // count (advanced by the job's chunk count).  Returns false after a wait
 // timeout (the CTA must then stop using the ring).
-template <int W, bool STAGED, bool CG = false>
+template <int W, bool STAGED, bool CG = false, int S = 1>
 __device__ __forceinline__ bool sample_tile(const SampleJob &j, const int64_t s0, uint64_t *bar, uint8_t *slots,
                                             uint32_t &g)
 {
     const int tid = threadIdx.x;
-    const int64_t s = s0 + tid;
-    const bool act = s < j.B;
     const int F = j.F;
-
-    uint64_t v[W];
+    // thread tid owns shots s0 + tid + r * blockDim.x, r < S
+    int64_t sh[S];
+    bool act[S];
+    bool any = false;
+    uint32_t live = 0;
+    uint64_t v[S][W];
 #pragma unroll
-    for (int w = 0; w < W; ++w) v[w] = 0;
-    if (act) {
-        const uint8_t *row = j.f + s * j.f_stride;
+    for (int r = 0; r < S; ++r) {
+        sh[r] = s0 + tid + (int64_t)r * blockDim.x;
+        act[r] = sh[r] < j.B;
+        any |= act[r];
+        live |= act[r] ? 1u << r : 0u;
 #pragma unroll
-        for (int w = 0; w < W; ++w) {
-            const int lim = min(64, F - 64 * w);
-            uint64_t x = 0;
-            for (int b = 0; b < lim; ++b) {
-                const int c = 64 * w + b;
-                const int col = j.f_sel ? ldj<CG>(j.f_sel + c) : c;
-                x |= (uint64_t)(ldj<CG>(row + col) & 1u) << b;
+        for (int w = 0; w < W; ++w) v[r][w] = 0;
+        if (act[r]) {
+            const uint8_t *row = j.f + sh[r] * j.f_stride;
+#pragma unroll
+            for (int w = 0; w < W; ++w) {
+                const int lim = min(64, F - 64 * w);
+                uint64_t x = 0;
+                for (int b = 0; b < lim; ++b) {
+                    const int c = 64 * w + b;
+                    const int col = j.f_sel ? ldj<CG>(j.f_sel + c) : c;
+                    x |= (uint64_t)(ldj<CG>(row + col) & 1u) << b;
+                }
+                v[r][w] = x;
             }
-            v[w] = x;
         }
     }
-    uint64_t vk[W];
-    graph_vector<W>(vk, v, F, 0, graph_params<CG>(j.gdir));
-    const uint64_t shot = (uint64_t)(j.shot_offset + s);
-    uint64_t rng = xorshift_init(j.seed, shot);
-    double prev = 0.0, sre = 0.0, sim = 0.0;
+    uint64_t vk[S][W];
+    {
+        const int P0 = graph_params<CG>(j.gdir);
+#pragma unroll
+        for (int r = 0; r < S; ++r) graph_vector<W>(vk[r], v[r], F, 0, P0);
+    }
+    uint64_t rng[S];
+    double prev[S], sre[S], sim[S];
+#pragma unroll
+    for (int r = 0; r < S; ++r) {
+        rng[r] = xorshift_init(j.seed, (uint64_t)(j.shot_offset + sh[r]));
+        prev[r] = 0.0;
+        sre[r] = 0.0;
+        sim[r] = 0.0;
+    }
     uint32_t flags = 0, risk = 0;
     const int nch = j.n_chunks;
 
@@ -225,29 +244,39 @@ __device__ __forceinline__ bool sample_tile(const SampleJob &j, const int64_t s0
         } else {
             p = j.image + d.off;
         }
-        if (act) eval_terms<W>(p, (uint32_t)d.n_terms, vk, sre, sim, risk);
+        if (any) eval_terms_s<W, S>(p, (uint32_t)d.n_terms, vk, sre, sim, risk, live);
         if (d.end_of_graph) {
             const int k = d.graph;
-            if (act) {
-                const double mag = dsqrt(dadd(dmul(sre, sre), dmul(sim, sim)));
-                if (j.amp) j.amp[s * (int64_t)(j.n_out + 1) + k] = mag;
+#pragma unroll
+            for (int r = 0; r < S; ++r) {
+                if (!act[r]) continue;
+                const double mag = dsqrt(dadd(dmul(sre[r], sre[r]), dmul(sim[r], sim[r])));
+                if (j.amp) j.amp[sh[r] * (int64_t)(j.n_out + 1) + k] = mag;
                 if (k == 0) {
-                    prev = mag;
+                    prev[r] = mag;
                 } else {
                     const int i = k - 1;
-                    const double u = j.rng_mode == KSIM_RNG_PHILOX ? philox_uniform(j.seed, shot, (uint32_t)i)
-                                                                   : xorshift_uniform(rng);
-                    const double ratio = __ddiv_rn(mag, prev);
+                    const double u = j.rng_mode == KSIM_RNG_PHILOX
+                                         ? philox_uniform(j.seed, (uint64_t)(j.shot_offset + sh[r]), (uint32_t)i)
+                                         : xorshift_uniform(rng[r]);
+                    const double ratio = __ddiv_rn(mag, prev[r]);
                     const uint32_t bit = u < ratio ? 1u : 0u;
-                    if (!(prev > 0.0)) flags |= KSIM_FLAG_PREV_NONPOSITIVE;
+                    if (!(prev[r] > 0.0)) flags |= KSIM_FLAG_PREV_NONPOSITIVE;
                     if (ratio != ratio) flags |= KSIM_FLAG_NAN;
-                    set_bit<W>(v, F + i, bit);
-                    prev = bit ? mag : dsub(prev, mag);
+                    set_bit<W>(v[r], F + i, bit);
+                    prev[r] = bit ? mag : dsub(prev[r], mag);
                 }
             }
-            sre = 0.0;
-            sim = 0.0;
-            if (k + 1 < j.n_graphs) graph_vector<W>(vk, v, F, k + 1, graph_params<CG>(j.gdir + k + 1));
+#pragma unroll
+            for (int r = 0; r < S; ++r) {
+                sre[r] = 0.0;
+                sim[r] = 0.0;
+            }
+            if (k + 1 < j.n_graphs) {
+                const int Pk = graph_params<CG>(j.gdir + k + 1);
+#pragma unroll
+                for (int r = 0; r < S; ++r) graph_vector<W>(vk[r], v[r], F, k + 1, Pk);
+            }
         }
         if (STAGED) {
             __syncthreads();
@@ -256,12 +285,16 @@ __device__ __forceinline__ bool sample_tile(const SampleJob &j, const int64_t s0
     }
     g += (uint32_t)nch;
 
-    if (act) {
-        uint8_t *orow = j.out + s * j.out_stride;
+#pragma unroll
+    for (int r = 0; r < S; ++r) {
+        if (!act[r]) continue;
+        uint8_t *orow = j.out + sh[r] * j.out_stride;
         for (int i = 0; i < j.n_out; ++i) {
             const int64_t col = j.out_cols ? (int64_t)ldj<CG>(j.out_cols + i) : j.out_col0 + i;
-            orow[col] = (uint8_t)get_bit<W>(v, F + i);
+            orow[col] = (uint8_t)get_bit<W>(v[r], F + i);
         }
+    }
+    if (any) {
         const uint32_t st = flags | (risk ? (uint32_t)KSIM_FLAG_INT64_RISK : 0u);
         if (st) atomicOr(j.status, st);
     }

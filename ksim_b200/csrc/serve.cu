@@ -97,7 +97,7 @@ __device__ __forceinline__ T vload(const T *p)
     return *(const volatile T *)p;
 }
 
-__global__ void __launch_bounds__(256) k_serve(ServeJob *jobs, ServeReqDev *reqs, const unsigned long long *ring,
+__global__ void __launch_bounds__(256, KSIM_SAMPLE_MIN_CTAS) k_serve(ServeJob *jobs, ServeReqDev *reqs, const unsigned long long *ring,
                                                int ring_cap, ServeCtl *ctl, uint32_t *done_flags, long long idle_ns)
 {
     extern __shared__ __align__(128) uint8_t smem[];
@@ -154,13 +154,14 @@ __global__ void __launch_bounds__(256) k_serve(ServeJob *jobs, ServeReqDev *reqs
         }
         __syncthreads();
         if (slot >= 0) {
-            const int64_t s0 = (int64_t)s_tile * blockDim.x;
+            constexpr int S = shots_per_thread(4);  // every loop job has W <= 4
+            const int64_t s0 = (int64_t)s_tile * blockDim.x * S;
             bool ok;
             switch (s_W) {
-            case 1: ok = sample_tile<1, true, true>(s_job, s0, bar, slots, g); break;
-            case 2: ok = sample_tile<2, true, true>(s_job, s0, bar, slots, g); break;
-            case 3: ok = sample_tile<3, true, true>(s_job, s0, bar, slots, g); break;
-            default: ok = sample_tile<4, true, true>(s_job, s0, bar, slots, g); break;
+            case 1: ok = sample_tile<1, true, true, S>(s_job, s0, bar, slots, g); break;
+            case 2: ok = sample_tile<2, true, true, S>(s_job, s0, bar, slots, g); break;
+            case 3: ok = sample_tile<3, true, true, S>(s_job, s0, bar, slots, g); break;
+            default: ok = sample_tile<4, true, true, S>(s_job, s0, bar, slots, g); break;
             }
             __threadfence();  // this thread's outputs before the counters below
             __syncthreads();
@@ -326,7 +327,8 @@ ksim_status admit(ksim_server *s, ServeRequest *r)
         return KSIM_OK;
     }
     // job descriptors
-    const int64_t tiles = (r->B + s->lcfg.threads - 1) / s->lcfg.threads;
+    const int64_t tile = (int64_t)s->lcfg.threads * shots_per_thread(4);
+    const int64_t tiles = (r->B + tile - 1) / tile;
     std::vector<int> new_jobs;
     for (size_t k = 0; k < p->parts.size(); ++k) {
         ksim_component *c = p->parts[k].comp;

@@ -273,16 +273,23 @@ struct TermOut {
 // (T = uint64_t) or that every value it must know exactly stays below 2^31
 // (T = uint32_t, TF_NARROW): adds and multiplies wrap, so intermediate sums
 // may leave the narrow range, but the values at each halving and at the end
-// are the true ones.
-template <int W, typename T = uint64_t>
-KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const uint64_t (&v)[W],
-                                    TermOut &o)
+// are the true ones.  S shots at once: each column record is loaded and
+// decoded once and applied to S independent parameter vectors.
+template <int W, typename T, int S>
+KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const uint64_t (&v)[S][W],
+                                    TermOut (&o)[S])
 {
     constexpr int R1 = rec1_words(W), R2 = rec2_words(W);
     const uint64_t *q = (const uint64_t *)(p + TERM_HDR_BYTES + ((h.flags & TF_APX) ? TERM_APX_BYTES : 0));
-    Zr<T> z = {1, 0, 0, 0};
-    int64_t pw = 0;
-    uint32_t alive = 1;
+    Zr<T> z[S];
+    int64_t pw[S];
+    uint32_t alive[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        z[s].a = 1; z[s].b = 0; z[s].c = 0; z[s].d = 0;
+        pw[s] = 0;
+        alive[s] = 1;
+    }
 
     // NodePhases
     for (uint32_t t = 0; t < h.n_np; ++t, q += R1) {
@@ -292,39 +299,57 @@ KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const ui
 #pragma unroll
         for (int w = 0; w < W; ++w) mw[w] = r[w];
         const uint32_t cw = (uint32_t)r[W];
-        const uint32_t neg = (parity<W>(mw, v) ^ (cw >> 2)) & 1u;
-        const uint32_t j = cw & 3u;
+        const uint32_t j = cw & 3u, c2 = (cw >> 2) & 1u;
+        uint32_t neg[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) neg[s] = parity<W>(mw, v[s]) ^ c2;
         if (j == 0) {
             // factor 2 (halved straight back, pw + 1) or 0 (the term dies)
-            pw += alive & (neg ^ 1u);
-            alive &= neg ^ 1u;
-            const T keep = (T)0 - (T)alive;
-            z.a &= keep; z.b &= keep; z.c &= keep; z.d &= keep;
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                pw[s] += alive[s] & (neg[s] ^ 1u);
+                alive[s] &= neg[s] ^ 1u;
+                const T keep = (T)0 - (T)alive[s];
+                z[s].a &= keep; z[s].b &= keep; z[s].c &= keep; z[s].d &= keep;
+            }
         } else {
-            const Zr<T> t0 = z;
-            add_rot(z, t0, j, (T)0 - (T)neg);
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const Zr<T> t0 = z[s];
+                add_rot(z[s], t0, j, (T)0 - (T)neg[s]);
+            }
             if (cw & NP_REDUCE_BIT) {
-                shr_all(z, 1u);
-                pw += alive;
+#pragma unroll
+                for (int s = 0; s < S; ++s) {
+                    shr_all(z[s], 1u);
+                    pw[s] += alive[s];
+                }
             }
         }
     }
     // HalfPi: w^(sum par*coeff); its renormalisation cannot fire (nu < 4 here)
     {
-        uint32_t tot = 0;
+        uint32_t tot[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) tot[s] = 0;
         for (uint32_t t = 0; t < h.n_hp; ++t, q += R1) {
             uint64_t r[R1];
             load_rec<R1>(q, r);
             uint64_t mw[W];
 #pragma unroll
             for (int w = 0; w < W; ++w) mw[w] = r[w];
-            tot += parity<W>(mw, v) ? (uint32_t)r[W] : 0u;
+            const uint32_t coeff = (uint32_t)r[W];
+#pragma unroll
+            for (int s = 0; s < S; ++s) tot[s] += parity<W>(mw, v[s]) ? coeff : 0u;
         }
-        z = rot_var(z, tot & 7u);
+#pragma unroll
+        for (int s = 0; s < S; ++s) z[s] = rot_var(z[s], tot[s] & 7u);
     }
     // PiProducts: overall sign
     {
-        uint32_t e = 0;
+        uint32_t e[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) e[s] = 0;
         for (uint32_t t = 0; t < h.n_pp; ++t, q += R2) {
             uint64_t r[R2];
             load_rec<R2>(q, r);
@@ -332,16 +357,24 @@ KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const ui
 #pragma unroll
             for (int w = 0; w < W; ++w) { ma[w] = r[w]; mb[w] = r[W + w]; }
             const uint32_t cw = (uint32_t)r[2 * W];
-            const uint32_t psi = (cw ^ parity<W>(ma, v)) & 1u;
-            const uint32_t phi = ((cw >> 1) ^ parity<W>(mb, v)) & 1u;
-            e ^= psi & phi;
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const uint32_t psi = (cw ^ parity<W>(ma, v[s])) & 1u;
+                const uint32_t phi = ((cw >> 1) ^ parity<W>(mb, v[s])) & 1u;
+                e[s] ^= psi & phi;
+            }
         }
-        const T m = (T)0 - (T)e;
-        z.a = sneg(z.a, m); z.b = sneg(z.b, m); z.c = sneg(z.c, m); z.d = sneg(z.d, m);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const T m = (T)0 - (T)e[s];
+            z[s].a = sneg(z[s].a, m); z[s].b = sneg(z[s].b, m); z[s].c = sneg(z[s].c, m); z[s].d = sneg(z[s].d, m);
+        }
     }
     // PhasePairs: per-shot valuation tracking
     {
-        uint32_t nu = h.nu_np;
+        uint32_t nu[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) nu[s] = h.nu_np;
         for (uint32_t t = 0; t < h.n_ph; ++t, q += R2) {
             uint64_t r[R2];
             load_rec<R2>(q, r);
@@ -349,34 +382,40 @@ KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const ui
 #pragma unroll
             for (int w = 0; w < W; ++w) { ma[w] = r[w]; mb[w] = r[W + w]; }
             const uint32_t cw = (uint32_t)r[2 * W];
-            const uint32_t pa = parity<W>(ma, v), pb = parity<W>(mb, v);
             const uint32_t ac = cw & 7u, bc = (cw >> 3) & 7u, gc = (ac + bc) & 7u;
-            const Zr<T> t0 = z;
-            add_rot(z, t0, ac & 3u, (T)0 - (T)(((ac >> 2) ^ pa) & 1u));
-            add_rot(z, t0, bc & 3u, (T)0 - (T)(((bc >> 2) ^ pb) & 1u));
-            add_rot(z, t0, gc & 3u, (T)0 - (T)(((gc >> 2) ^ pa ^ pb ^ 1u) & 1u));
-            const uint32_t nf = (cw >> (8 + 4 * (pa | (pb << 1)))) & 15u;
-            alive &= (nf != NU_ZERO) ? 1u : 0u;
-            nu += nf;
-            const uint32_t red = alive & (nu >= 4 ? 1u : 0u);
-            nu -= 4 * red;
-            shr_all(z, red);
-            pw += red;
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const uint32_t pa = parity<W>(ma, v[s]), pb = parity<W>(mb, v[s]);
+                const Zr<T> t0 = z[s];
+                add_rot(z[s], t0, ac & 3u, (T)0 - (T)(((ac >> 2) ^ pa) & 1u));
+                add_rot(z[s], t0, bc & 3u, (T)0 - (T)(((bc >> 2) ^ pb) & 1u));
+                add_rot(z[s], t0, gc & 3u, (T)0 - (T)(((gc >> 2) ^ pa ^ pb ^ 1u) & 1u));
+                const uint32_t nf = (cw >> (8 + 4 * (pa | (pb << 1)))) & 15u;
+                alive[s] &= (nf != NU_ZERO) ? 1u : 0u;
+                nu[s] += nf;
+                const uint32_t red = alive[s] & (nu[s] >= 4 ? 1u : 0u);
+                nu[s] -= 4 * red;
+                shr_all(z[s], red);
+                pw[s] += red;
+            }
         }
     }
     // prefactor: w^idx, then the exact floatfactor with one renormalisation
-    z = rot_var(z, h.pf_idx);
     const Zr<T> ff = {(T)h.ff.a, (T)h.ff.b, (T)h.ff.c, (T)h.ff.d};
-    z = zmul(z, ff);
-    zreduce(z, pw);
-    if constexpr (sizeof(T) == 8) {
-        o.z = z;
-    } else {
-        o.z = widen(z);
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        Zr<T> zz = rot_var(z[s], h.pf_idx);
+        zz = zmul(zz, ff);
+        zreduce(zz, pw[s]);
+        if constexpr (sizeof(T) == 8) {
+            o[s].z = zz;
+        } else {
+            o[s].z = widen(zz);
+        }
+        o[s].pw = pw[s];
+        o[s].power2 = h.power2;
+        o[s].risk = 0;
     }
-    o.pw = pw;
-    o.power2 = h.power2;
-    o.risk = 0;
     return (const uint8_t *)q;
 }
 
@@ -462,33 +501,62 @@ KS_HD void term_complex(const TermOut &o, const uint8_t *hdr_ptr, uint32_t flags
     }
 }
 
-// One term on the path its header selects.  Returns the next record.
+// One term for S shots on the path its header selects.  Returns the next record.
+template <int W, int S>
+KS_HD const uint8_t *eval_term_s(const uint8_t *p, const TermHdr &h, const uint64_t (&v)[S][W],
+                                 TermOut (&o)[S])
+{
+    if (h.flags & TF_SLOW) {
+        const uint8_t *next = p;
+#pragma unroll
+        for (int s = 0; s < S; ++s) next = eval_term_exact<W>(p, h, v[s], o[s]);
+        return next;
+    }
+    if (h.flags & TF_NARROW) return eval_term_fast<W, uint32_t, S>(p, h, v, o);
+    return eval_term_fast<W, uint64_t, S>(p, h, v, o);
+}
+
+// One term for one shot.
 template <int W>
 KS_HD const uint8_t *eval_term(const uint8_t *p, const TermHdr &h, const uint64_t (&v)[W], TermOut &o)
 {
-    if (h.flags & TF_SLOW) return eval_term_exact<W>(p, h, v, o);
-    if (h.flags & TF_NARROW) return eval_term_fast<W, uint32_t>(p, h, v, o);
-    return eval_term_fast<W, uint64_t>(p, h, v, o);
+    return eval_term_s<W, 1>(p, h, reinterpret_cast<const uint64_t(&)[1][W]>(v),
+                             reinterpret_cast<TermOut(&)[1]>(o));
 }
 
-// Evaluate `n_terms` consecutive term records starting at p, adding their
-// complex values to (sum_re, sum_im) in order.  Returns the end pointer.
-template <int W>
-KS_HD const uint8_t *eval_terms(const uint8_t *p, uint32_t n_terms, const uint64_t (&v)[W],
-                                double &sum_re, double &sum_im, uint32_t &risk)
+// Evaluate `n_terms` consecutive term records starting at p for S shots,
+// adding each term's complex value to (sum_re[s], sum_im[s]) in order.
+// Risk flags count only for the shots set in `live`.  Returns the end pointer.
+template <int W, int S>
+KS_HD const uint8_t *eval_terms_s(const uint8_t *p, uint32_t n_terms, const uint64_t (&v)[S][W],
+                                  double (&sum_re)[S], double (&sum_im)[S], uint32_t &risk,
+                                  uint32_t live = ~0u)
 {
     for (uint32_t t = 0; t < n_terms; ++t) {
         const TermHdr h = load_hdr(p);
-        TermOut o;
-        const uint8_t *next = eval_term<W>(p, h, v, o);
-        double re, im;
-        term_complex(o, p, h.flags, re, im);
-        sum_re = dadd(sum_re, re);
-        sum_im = dadd(sum_im, im);
-        risk |= o.risk;
+        TermOut o[S];
+        const uint8_t *next = eval_term_s<W, S>(p, h, v, o);
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            double re, im;
+            term_complex(o[s], p, h.flags, re, im);
+            sum_re[s] = dadd(sum_re[s], re);
+            sum_im[s] = dadd(sum_im[s], im);
+            risk |= o[s].risk & (live >> s);
+        }
         p = next;
     }
     return p;
+}
+
+// The same for one shot.
+template <int W>
+KS_HD const uint8_t *eval_terms(const uint8_t *p, uint32_t n_terms, const uint64_t (&v)[W], double &sum_re,
+                                double &sum_im, uint32_t &risk)
+{
+    return eval_terms_s<W, 1>(p, n_terms, reinterpret_cast<const uint64_t(&)[1][W]>(v),
+                              reinterpret_cast<double(&)[1]>(sum_re), reinterpret_cast<double(&)[1]>(sum_im),
+                              risk);
 }
 
 // Parameter-vector masks: bits [lo, hi) of word w.

@@ -44,28 +44,31 @@ class HostEmu:
         self.n = len(self.graphs)
 
     def stats(self) -> dict:
-        st = np.zeros(5, np.int64)
+        st = np.zeros(6, np.int64)
         rc = self.L.hostemu_stats(self.descs, self.n, self.F, st.ctypes.data)
         if rc:
             raise ValueError(self.L.hostemu_error().decode())
-        return dict(zip(("W", "terms", "slow_terms", "columns", "max_term_bytes"), st.tolist()))
+        return dict(zip(("W", "terms", "slow_terms", "columns", "max_term_bytes", "narrow_terms"),
+                        st.tolist()))
 
-    def eval(self, gi, params) -> np.ndarray:
+    def eval(self, gi, params, pairs: bool = False) -> np.ndarray:
+        """Complex amplitudes; pairs=True evaluates two rows at a time (the
+        two-shots-per-thread path of the kernels)."""
         p = np.ascontiguousarray(params, np.uint8)
         out = np.zeros((p.shape[0], 2))
         rc = self.L.hostemu_eval(self.descs, self.n, self.F, gi,
                                  p.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), p.shape[0],
-                                 p.shape[1], 0, out.ctypes.data, None)
+                                 p.shape[1], 4 if pairs else 0, out.ctypes.data, None)
         assert rc == 0, self.L.hostemu_error()
         return out[:, 0] + 1j * out[:, 1]
 
-    def eval_terms(self, gi, params) -> np.ndarray:
+    def eval_terms(self, gi, params, pairs: bool = False) -> np.ndarray:
         p = np.ascontiguousarray(params, np.uint8)
         G = int(np.asarray(self.graphs[gi]["pf_phase_idx"]).shape[0])
         out = np.zeros((p.shape[0], G, 5), np.int64)
         rc = self.L.hostemu_eval(self.descs, self.n, self.F, gi,
                                  p.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), p.shape[0],
-                                 p.shape[1], 2, out.ctypes.data, None)
+                                 p.shape[1], 3 if pairs else 2, out.ctypes.data, None)
         assert rc == 0, self.L.hostemu_error()
         return out
 

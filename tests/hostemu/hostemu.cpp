@@ -27,10 +27,52 @@ void pack_row(const uint8_t *row, int64_t n, uint64_t (&v)[W])
     for (int64_t c = 0; c < n && c < 64 * W; ++c) v[c >> 6] |= (uint64_t)(row[c] & 1u) << (c & 63);
 }
 
+// Modes 3 (per-term numerators) and 4 (complex amplitude): the same as 2 and
+// 0, evaluated two rows at a time through the two-shots-per-thread path.
+template <int W>
+void eval_rows_pairs(const HostImage &img, int gi, const uint8_t *params, int64_t B, int64_t P, int mode,
+                     void *out, uint32_t *risk_out)
+{
+    const GraphDir &gd = img.gdir[gi];
+    uint32_t risk = 0;
+    for (int64_t s = 0; s < B; s += 2) {
+        const int n = B - s >= 2 ? 2 : 1;
+        uint64_t v[2][W];
+        pack_row<W>(params + s * P, P, v[0]);
+        pack_row<W>(params + (s + n - 1) * P, P, v[1]);
+        const uint8_t *p = img.bytes.data() + gd.stream_off;
+        if (mode == 3) {
+            for (int t = 0; t < gd.G; ++t) {
+                const TermHdr h = load_hdr(p);
+                TermOut r[2];
+                p = eval_term_s<W, 2>(p, h, v, r);
+                for (int k = 0; k < n; ++k) {
+                    int64_t *o = (int64_t *)out + (s + k) * (int64_t)gd.G * 5 + 5 * t;
+                    o[0] = (int64_t)r[k].z.a;
+                    o[1] = (int64_t)r[k].z.b;
+                    o[2] = (int64_t)r[k].z.c;
+                    o[3] = (int64_t)r[k].z.d;
+                    o[4] = r[k].pw;
+                    risk |= r[k].risk;
+                }
+            }
+        } else {
+            double re[2] = {0, 0}, im[2] = {0, 0};
+            eval_terms_s<W, 2>(p, (uint32_t)gd.G, v, re, im, risk, n == 2 ? 3u : 1u);
+            for (int k = 0; k < n; ++k) {
+                ((double *)out)[2 * (s + k)] = re[k];
+                ((double *)out)[2 * (s + k) + 1] = im[k];
+            }
+        }
+    }
+    if (risk_out) *risk_out = risk;
+}
+
 template <int W>
 void eval_rows(const HostImage &img, int gi, const uint8_t *params, int64_t B, int64_t P, int mode,
                void *out, uint32_t *risk_out)
 {
+    if (mode >= 3) return eval_rows_pairs<W>(img, gi, params, B, P, mode, out, risk_out);
     const GraphDir &gd = img.gdir[gi];
     uint32_t risk = 0;
     for (int64_t s = 0; s < B; ++s) {
@@ -114,7 +156,7 @@ extern "C" {
 
 const char *hostemu_error(void) { return g_err.c_str(); }
 
-// stats: [W, n_terms, n_slow_terms, n_columns, max_term_bytes]
+// stats: [W, n_terms, n_slow_terms, n_columns, max_term_bytes, n_narrow_terms]
 int hostemu_stats(const ksim_graph_desc *g, int n, int F, int64_t *stats)
 {
     HostImage img;
@@ -125,6 +167,7 @@ int hostemu_stats(const ksim_graph_desc *g, int n, int F, int64_t *stats)
     stats[2] = img.n_slow_terms;
     stats[3] = img.n_columns;
     stats[4] = img.max_term_bytes;
+    stats[5] = img.n_narrow_terms;
     return 0;
 }
 
