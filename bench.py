@@ -492,18 +492,30 @@ def main():
     value = world * shots * args.steps / (total_ms / 1e3)
     ms_per_step = total_ms / args.steps
 
-    # end to end through the drop-in API from pinned host memory
+    # end to end through the drop-in API, pinned host buffers in and out
     f_pin = torch.from_numpy(f).pin_memory().numpy()
+    out_pin = torch.empty((shots, n_out), dtype=torch.uint8).pin_memory().numpy()
     for i in range(max(1, args.warmup)):
-        sampler.sample(f_pin, 3000 + i, rng_mode=args.rng)
+        sampler.sample(f_pin, 3000 + i, rng_mode=args.rng, out=out_pin)
     barrier(world)
     e2e_t = []
     for i in range(args.steps):
         t0 = time.perf_counter()
-        out = sampler.sample(f_pin, 4000 + i, rng_mode=args.rng)
+        sampler.sample(f_pin, 4000 + i, rng_mode=args.rng, out=out_pin)
         e2e_t.append(time.perf_counter() - t0)
     e2e_total = max_over_ranks(sum(e2e_t), world)
     e2e_value = world * shots * args.steps / e2e_total
+    # the same through the bit-packed entry point (8 f columns / outputs per byte)
+    fp_pin = torch.from_numpy(np.packbits(f, axis=1, bitorder="little")).pin_memory().numpy()
+    for i in range(max(1, args.warmup)):
+        sampler.sample_packed(fp_pin, n_f, 3000 + i, rng_mode=args.rng)
+    barrier(world)
+    e2p_t = []
+    for i in range(args.steps):
+        t0 = time.perf_counter()
+        sampler.sample_packed(fp_pin, n_f, 4000 + i, rng_mode=args.rng)
+        e2p_t.append(time.perf_counter() - t0)
+    e2p_value = world * shots * args.steps / max_over_ranks(sum(e2p_t), world)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -534,7 +546,12 @@ def main():
                        "l2": "flushed between steps (256 MiB write)",
                        "parallelism": f"shot-split x{world}"},
             "e2e": {"value": e2e_value, "unit": "shots/s", "h2d_bytes_per_step": int(f.nbytes),
-                    "d2h_bytes_per_step": int(shots * n_out)},
+                    "d2h_bytes_per_step": int(shots * n_out),
+                    "api": "B200ProgramSampler.sample (ksim_program_sample), pinned buffers"},
+            "e2e_packed": {"value": e2p_value, "unit": "shots/s",
+                           "h2d_bytes_per_step": int(fp_pin.nbytes),
+                           "d2h_bytes_per_step": int(shots * ((n_out + 7) // 8)),
+                           "api": "B200ProgramSampler.sample_packed (ksim_program_sample_packed)"},
             "roofline": {"bound": "alu", "achieved": achieved / 1e9, "peak": peak.value / 1e9,
                          "unit": "Gop/s (int32)", "frac": achieved / peak.value,
                          "traffic": (NCU_DRAM_BYTES_PER_SHOT[w.name] * shots

@@ -205,9 +205,19 @@ int32_t ksim_program_min_f_cols(const ksim_program *p);
 /* f_params: (B, n_f_cols) uint8 host; out: (B, n_outputs) uint8 host.
  * Component k is seeded with seed + 0x9E37*k and the outputs are permuted by
  * argsort(output_order), as sampler.py:57-67 does; the f_selection gather and
- * the permutation run on the device. */
+ * the permutation run on the device.  Large calls are split into chunks of
+ * shots whose copies overlap the sampling of their neighbours (page-locked
+ * host buffers let the copies run asynchronously). */
 ksim_status ksim_program_sample(ksim_program *p, const uint8_t *f_params, int64_t B,
                                 int64_t n_f_cols, uint64_t seed, int32_t rng_mode, uint8_t *out);
+/* Bit-packed host I/O (no reference counterpart; it cuts the PCIe bytes of
+ * ksim_program_sample 8x): f_packed has B rows of ceil(n_f_cols/8) bytes and
+ * out_packed B rows of ceil(n_outputs/8) bytes; column c of a row is bit c%8
+ * of byte c/8 (numpy.packbits(..., bitorder="little")).  The bits are those of
+ * ksim_program_sample. */
+ksim_status ksim_program_sample_packed(ksim_program *p, const uint8_t *f_packed, int64_t B,
+                                       int64_t n_f_cols, uint64_t seed, int32_t rng_mode,
+                                       uint8_t *out_packed);
 /* Same on device buffers, asynchronous on `stream`. */
 ksim_status ksim_program_sample_device(ksim_program *p, const uint8_t *d_f_params, int64_t B,
                                        int64_t n_f_cols, int64_t shot_offset, uint64_t seed,

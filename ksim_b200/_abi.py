@@ -215,6 +215,7 @@ def _declare(L: ctypes.CDLL) -> None:
         "ksim_program_min_f_cols": (i32, [vp]),
         "ksim_program_sample": (i32, [vp, _u8p, i64, i64, u64, i32, _u8p]),
         "ksim_program_sample_device": (i32, [vp, vp, i64, i64, i64, u64, i32, vp, vp]),
+        "ksim_program_sample_packed": (i32, [vp, _u8p, i64, i64, u64, i32, _u8p]),
         "ksim_measure_int_peak": (i32, [i32, dp, dp]),
         "ksim_batch_create": (i32, [ctypes.POINTER(BatchJob), i32, ctypes.POINTER(BatchTuning),
                                     ctypes.POINTER(vp)]),

@@ -462,10 +462,12 @@ ksim_status ksim_program_create(ksim_component *const *comps, int32_t n_comps, c
         }
         off += n;
     }
-    cudaError_t e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
-    if (e != cudaSuccess) {
-        ksim_program_destroy(p.release());
-        return cuda_fail(e, "cudaStreamCreate");
+    for (cudaStream_t *st : {&p->stream, &p->stream_b, &p->s_h2d, &p->s_d2h}) {
+        cudaError_t e = cudaStreamCreateWithFlags(st, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            ksim_program_destroy(p.release());
+            return cuda_fail(e, "cudaStreamCreate");
+        }
     }
     *out = p.release();
     return KSIM_OK;
@@ -475,14 +477,18 @@ void ksim_program_destroy(ksim_program *p)
 {
     if (!p) return;
     DeviceGuard g(p->device);
-    if (p->stream) cudaStreamSynchronize(p->stream);
+    for (cudaStream_t st : {p->stream, p->stream_b, p->s_h2d, p->s_d2h})
+        if (st) cudaStreamSynchronize(st);
     for (auto &part : p->parts) {
         if (part.d_sel) cudaFree(part.d_sel);
         if (part.d_cols) cudaFree(part.d_cols);
     }
     p->ws_f.release();
     p->ws_out.release();
-    if (p->stream) cudaStreamDestroy(p->stream);
+    p->ws_fp.release();
+    p->ws_op.release();
+    for (cudaStream_t st : {p->stream, p->stream_b, p->s_h2d, p->s_d2h})
+        if (st) cudaStreamDestroy(st);
     delete p;
 }
 
@@ -555,29 +561,88 @@ ksim_status ksim_program_sample_device(ksim_program *p, const uint8_t *d_f_param
     return KSIM_OK;
 }
 
-ksim_status ksim_program_sample(ksim_program *p, const uint8_t *f_params, int64_t B, int64_t n_f_cols,
-                                uint64_t seed, int32_t rng_mode, uint8_t *out)
+}  // extern "C"
+
+namespace {
+
+// Host buffers in, host buffers out, in chunks of shots pipelined over four
+// streams: the f rows of chunk i+1 cross PCIe while chunk i samples, the
+// results of chunk i cross back while chunk i+1 samples, and consecutive
+// chunks alternate between two compute streams so one chunk's last wave of
+// CTAs overlaps the next chunk's first.  Chunk c samples with shot_offset =
+// its first row, so the bits equal a single launch over all B shots.
+// packed: f rows of ceil(n_f_cols/8) bytes and output rows of
+// ceil(n_outputs/8) bytes, bit c of a row in byte c/8 at bit c%8.
+ksim_status program_sample_host(ksim_program *p, const uint8_t *f, int64_t B, int64_t n_f_cols, uint64_t seed,
+                                int32_t rng_mode, uint8_t *out, bool packed)
 {
     if (!p) return fail(KSIM_ERR_INVALID_ARGUMENT, "program is NULL");
     if (B < 0 || n_f_cols < 0) return fail(KSIM_ERR_INVALID_ARGUMENT, "B and n_f_cols must be >= 0");
     if (B == 0 || p->n_outputs == 0) return check_rng(rng_mode);
-    if ((n_f_cols > 0 && !f_params) || !out) return fail(KSIM_ERR_INVALID_ARGUMENT, "NULL buffer");
+    if ((n_f_cols > 0 && !f) || !out) return fail(KSIM_ERR_INVALID_ARGUMENT, "NULL buffer");
+    if (check_rng(rng_mode) != KSIM_OK) return KSIM_ERR_INVALID_ARGUMENT;
+    if (n_f_cols < p->min_f_cols)
+        return fail(KSIM_ERR_INVALID_ARGUMENT, "f_params has " + std::to_string(n_f_cols) +
+                                                   " columns; f_selection needs " + std::to_string(p->min_f_cols));
     DeviceGuard g(p->device);
     std::lock_guard<std::mutex> lk(p->mu);
+    const int64_t n_out = p->n_outputs;
+    const int64_t f_row = packed ? (n_f_cols + 7) / 8 : n_f_cols;
+    const int64_t o_row = packed ? (n_out + 7) / 8 : n_out;
     cudaError_t e = p->ws_f.ensure((size_t)std::max<int64_t>(B * n_f_cols, 1));
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(f workspace)");
-    e = p->ws_out.ensure((size_t)(B * p->n_outputs));
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(output workspace)");
-    if (n_f_cols > 0) {
-        e = cudaMemcpyAsync(p->ws_f.p, f_params, (size_t)(B * n_f_cols), cudaMemcpyHostToDevice, p->stream);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync(f)");
+    if (e == cudaSuccess) e = p->ws_out.ensure((size_t)(B * n_out));
+    if (e == cudaSuccess && packed) e = p->ws_fp.ensure((size_t)std::max<int64_t>(B * f_row, 1));
+    if (e == cudaSuccess && packed) e = p->ws_op.ensure((size_t)(B * o_row));
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(program workspace)");
+    uint8_t *d_f = (uint8_t *)p->ws_f.p, *d_out = (uint8_t *)p->ws_out.p;
+    uint8_t *d_in = packed ? (uint8_t *)p->ws_fp.p : d_f;       // where the host rows land
+    uint8_t *d_back = packed ? (uint8_t *)p->ws_op.p : d_out;   // what goes back
+
+    // chunks: about a quarter of the shots each, at least 128 Ki shots
+    const int64_t chunk = std::max<int64_t>((int64_t)1 << 17, ((B + 3) / 4 + 4095) / 4096 * 4096);
+    const int n_chunks = (int)((B + chunk - 1) / chunk);
+    std::vector<cudaEvent_t> ev_in(n_chunks, nullptr), ev_done(n_chunks, nullptr);
+    ksim_status st = KSIM_OK;
+    for (int i = 0; i < n_chunks && e == cudaSuccess; ++i) {
+        e = cudaEventCreateWithFlags(&ev_in[i], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_done[i], cudaEventDisableTiming);
     }
-    ksim_status st = ksim_program_sample_device(p, (const uint8_t *)p->ws_f.p, B, n_f_cols, 0, seed, rng_mode,
-                                                (uint8_t *)p->ws_out.p, p->stream);
+    auto copy_back = [&](int i) -> cudaError_t {
+        const int64_t c0 = (int64_t)i * chunk, n = std::min(chunk, B - c0);
+        cudaError_t x = cudaStreamWaitEvent(p->s_d2h, ev_done[i], 0);
+        if (x == cudaSuccess)
+            x = cudaMemcpyAsync(out + c0 * o_row, d_back + c0 * o_row, (size_t)(n * o_row), cudaMemcpyDeviceToHost,
+                                p->s_d2h);
+        return x;
+    };
+    for (int i = 0; i < n_chunks && e == cudaSuccess && st == KSIM_OK; ++i) {
+        const int64_t c0 = (int64_t)i * chunk, n = std::min(chunk, B - c0);
+        cudaStream_t cs = (i & 1) ? p->stream_b : p->stream;
+        if (f_row > 0)
+            e = cudaMemcpyAsync(d_in + c0 * f_row, f + c0 * f_row, (size_t)(n * f_row), cudaMemcpyHostToDevice,
+                                p->s_h2d);
+        if (e == cudaSuccess) e = cudaEventRecord(ev_in[i], p->s_h2d);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, ev_in[i], 0);
+        if (e == cudaSuccess && packed)
+            e = launch_unpack_bits(d_in + c0 * f_row, n, f_row, n_f_cols, d_f + c0 * n_f_cols, cs);
+        if (e != cudaSuccess) break;
+        st = ksim_program_sample_device(p, d_f + c0 * n_f_cols, n, n_f_cols, c0, seed, rng_mode, d_out + c0 * n_out,
+                                        cs);
+        if (st != KSIM_OK) break;
+        if (packed) e = launch_pack_bits(d_out + c0 * n_out, n, n_out, o_row, d_back + c0 * o_row, cs);
+        if (e == cudaSuccess) e = cudaEventRecord(ev_done[i], cs);
+        if (e == cudaSuccess && i > 0) e = copy_back(i - 1);  // after chunk i is queued
+    }
+    if (e == cudaSuccess && st == KSIM_OK) e = copy_back(n_chunks - 1);
+    for (cudaStream_t x : {p->s_h2d, p->stream, p->stream_b, p->s_d2h}) {
+        const cudaError_t y = cudaStreamSynchronize(x);
+        if (e == cudaSuccess) e = y;
+    }
+    for (int i = 0; i < n_chunks; ++i) {
+        if (ev_in[i]) cudaEventDestroy(ev_in[i]);
+        if (ev_done[i]) cudaEventDestroy(ev_done[i]);
+    }
     if (st != KSIM_OK) return st;
-    e = cudaMemcpyAsync(out, p->ws_out.p, (size_t)(B * p->n_outputs), cudaMemcpyDeviceToHost, p->stream);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync(out)");
-    e = cudaStreamSynchronize(p->stream);
     if (e != cudaSuccess) return cuda_fail(e, "program sample");
     for (auto &part : p->parts) {
         uint32_t flags = 0;
@@ -586,6 +651,22 @@ ksim_status ksim_program_sample(ksim_program *p, const uint8_t *f_params, int64_
         if (flags & KSIM_FLAG_WAIT_TIMEOUT) return fail(KSIM_ERR_TIMEOUT, "a staging wait timed out");
     }
     return KSIM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+ksim_status ksim_program_sample(ksim_program *p, const uint8_t *f_params, int64_t B, int64_t n_f_cols,
+                                uint64_t seed, int32_t rng_mode, uint8_t *out)
+{
+    return program_sample_host(p, f_params, B, n_f_cols, seed, rng_mode, out, false);
+}
+
+ksim_status ksim_program_sample_packed(ksim_program *p, const uint8_t *f_packed, int64_t B, int64_t n_f_cols,
+                                       uint64_t seed, int32_t rng_mode, uint8_t *out_packed)
+{
+    return program_sample_host(p, f_packed, B, n_f_cols, seed, rng_mode, out_packed, true);
 }
 
 }  // extern "C"

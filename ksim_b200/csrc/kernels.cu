@@ -103,7 +103,59 @@ cudaError_t launch_eval_w(const EvalJob &j, cudaStream_t st)
     return cudaGetLastError();
 }
 
+// One output byte per thread (grid-stride): HBM-bound byte work.
+__global__ void __launch_bounds__(256) k_unpack_bits(const uint8_t *__restrict__ packed, int64_t rows,
+                                                     int64_t packed_row, int64_t n_cols, uint8_t *__restrict__ out)
+{
+    const int64_t n = rows * n_cols;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = i / n_cols, c = i - r * n_cols;
+        out[i] = (packed[r * packed_row + (c >> 3)] >> (c & 7)) & 1u;
+    }
+}
+
+// One packed byte per thread (grid-stride).
+__global__ void __launch_bounds__(256) k_pack_bits(const uint8_t *__restrict__ bytes, int64_t rows, int64_t n_cols,
+                                                   int64_t packed_row, uint8_t *__restrict__ out)
+{
+    const int64_t n = rows * packed_row;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = i / packed_row, b = i - r * packed_row;
+        const uint8_t *src = bytes + r * n_cols + 8 * b;
+        const int64_t m = n_cols - 8 * b < 8 ? n_cols - 8 * b : 8;
+        uint32_t x = 0;
+        for (int k = 0; k < m; ++k) x |= (uint32_t)(src[k] & 1u) << k;
+        out[i] = (uint8_t)x;
+    }
+}
+
+unsigned byte_grid(int64_t n)
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t want = (n + 255) / 256;
+    const int64_t cap = (int64_t)sms * 8;
+    return (unsigned)(want < cap ? (want > 0 ? want : 1) : cap);
+}
+
 }  // namespace
+
+cudaError_t launch_unpack_bits(const uint8_t *packed, int64_t rows, int64_t packed_row, int64_t n_cols, uint8_t *out,
+                               cudaStream_t st)
+{
+    if (rows <= 0 || n_cols <= 0) return cudaSuccess;
+    k_unpack_bits<<<byte_grid(rows * n_cols), 256, 0, st>>>(packed, rows, packed_row, n_cols, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack_bits(const uint8_t *bytes, int64_t rows, int64_t n_cols, int64_t packed_row, uint8_t *out,
+                             cudaStream_t st)
+{
+    if (rows <= 0 || n_cols <= 0) return cudaSuccess;
+    k_pack_bits<<<byte_grid(rows * packed_row), 256, 0, st>>>(bytes, rows, n_cols, packed_row, out);
+    return cudaGetLastError();
+}
 
 size_t staged_smem_bytes(int slot_bytes) { return (size_t)BAR_BYTES + (size_t)NSLOT * (size_t)slot_bytes; }
 

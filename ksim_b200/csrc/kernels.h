@@ -65,6 +65,12 @@ struct EvalJob {
 
 cudaError_t launch_eval(const EvalJob &job, int W, cudaStream_t st);
 
+// Bit-packed rows (bit c of a row = byte c/8, bit c%8) <-> one byte per bit.
+cudaError_t launch_unpack_bits(const uint8_t *packed, int64_t rows, int64_t packed_row, int64_t n_cols,
+                               uint8_t *out, cudaStream_t st);
+cudaError_t launch_pack_bits(const uint8_t *bytes, int64_t rows, int64_t n_cols, int64_t packed_row,
+                             uint8_t *out, cudaStream_t st);
+
 // Shared-memory bytes the staged sampler needs for a slot size.
 size_t staged_smem_bytes(int slot_bytes);
 

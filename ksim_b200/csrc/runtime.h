@@ -65,8 +65,10 @@ struct ksim_program {
     int n_outputs = 0;
     int min_f_cols = 0;
     std::vector<ProgramPart> parts;
-    cudaStream_t stream = nullptr;
-    ksim::DevBuf ws_f, ws_out;
+    // host-buffer calls: two compute streams (chunk tails overlap) and one
+    // stream per copy direction
+    cudaStream_t stream = nullptr, stream_b = nullptr, s_h2d = nullptr, s_d2h = nullptr;
+    ksim::DevBuf ws_f, ws_out, ws_fp, ws_op;  // unpacked rows; bit-packed rows
     std::mutex mu;
 };
 
