@@ -516,6 +516,22 @@ def main():
         sampler.sample_packed(fp_pin, n_f, 4000 + i, rng_mode=args.rng)
         e2p_t.append(time.perf_counter() - t0)
     e2p_value = world * shots * args.steps / max_over_ranks(sum(e2p_t), world)
+    # f drawn on the device from a Pauli noise model of the workload's shape
+    # (one channel per gate location), then sampled: only outputs cross PCIe
+    from ksim_b200 import synth
+    from ksim_b200.noise import DeviceChannelSampler
+    nprobs, nT = synth.noise_model(np.random.default_rng(w.seed + 7), n_f, 200)
+    noise = DeviceChannelSampler(nprobs, nT, seed=w.seed, device=local)
+    for i in range(max(1, args.warmup)):
+        sampler.sample_noisy(noise, shots, 3000 + i, rng_mode=args.rng, out=out_pin)
+    barrier(world)
+    e2n_t = []
+    for i in range(args.steps):
+        t0 = time.perf_counter()
+        sampler.sample_noisy(noise, shots, 4000 + i, noise_seed=rank * 1000 + i, rng_mode=args.rng,
+                             out=out_pin)
+        e2n_t.append(time.perf_counter() - t0)
+    e2n_value = world * shots * args.steps / max_over_ranks(sum(e2n_t), world)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -548,6 +564,10 @@ def main():
             "e2e": {"value": e2e_value, "unit": "shots/s", "h2d_bytes_per_step": int(f.nbytes),
                     "d2h_bytes_per_step": int(shots * n_out),
                     "api": "B200ProgramSampler.sample (ksim_program_sample), pinned buffers"},
+            "e2e_noisy": {"value": e2n_value, "unit": "shots/s", "h2d_bytes_per_step": 0,
+                          "d2h_bytes_per_step": int(shots * n_out),
+                          "api": "B200ProgramSampler.sample_noisy (ksim_program_sample_noisy): "
+                                 "f drawn on the device from 200 Pauli channels"},
             "e2e_packed": {"value": e2p_value, "unit": "shots/s",
                            "h2d_bytes_per_step": int(fp_pin.nbytes),
                            "d2h_bytes_per_step": int(shots * ((n_out + 7) // 8)),

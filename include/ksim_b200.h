@@ -223,6 +223,37 @@ ksim_status ksim_program_sample_device(ksim_program *p, const uint8_t *d_f_param
                                        int64_t n_f_cols, int64_t shot_offset, uint64_t seed,
                                        int32_t rng_mode, uint8_t *d_out, void *stream);
 
+/* ---- noise: the f parameters drawn on the device ------------------------ */
+
+/* A noise model: ChannelSampler(channel_probs, error_transform)
+ * (src/python/ksim/compile/channels.py:531-576).  Channel i has n_bits[i]
+ * error bits and 2^n_bits[i] outcome probabilities, concatenated in `probs`
+ * (outcome index bit b = error bit b, channels.py:12-24); error_transform is
+ * (num_f, num_e) uint8 row-major, num_e = sum of n_bits.  The draw
+ * (ChannelSampler.sample, channels.py:624-658) runs one thread per shot over
+ * all channels with counter-based Philox4x32-10 draws keyed by (seed, shot):
+ * channel c fires iff u32(shot, c) < floor(p_fire 2^32), the outcome is the
+ * first whose conditional-CDF threshold exceeds a second draw, and its f
+ * pattern is XORed in. */
+typedef struct ksim_noise ksim_noise;
+ksim_status ksim_noise_create(const double *probs, const int32_t *n_bits, int32_t n_channels,
+                              const uint8_t *error_transform, int32_t num_f, int32_t num_e,
+                              int32_t device, ksim_noise **out);
+void ksim_noise_destroy(ksim_noise *n);
+int32_t ksim_noise_num_f(const ksim_noise *n);
+int32_t ksim_noise_num_channels(const ksim_noise *n);   /* channels that can fire */
+/* f rows (B x num_f bytes, f_stride apart) for shots shot_offset.. on the device. */
+ksim_status ksim_noise_sample_device(ksim_noise *n, int64_t B, int64_t shot_offset, uint64_t seed,
+                                     uint8_t *d_f, int64_t f_stride, void *stream);
+/* The same into host memory (B x num_f bytes), synchronous. */
+ksim_status ksim_noise_sample(ksim_noise *n, int64_t B, int64_t shot_offset, uint64_t seed,
+                              uint8_t *f_host);
+/* Draw f on the device and sample program p from it: only the outputs
+ * (B x n_outputs bytes, host) cross PCIe.  Equals
+ * ksim_program_sample(p, f, ...) with f = ksim_noise_sample(n, B, 0, noise_seed). */
+ksim_status ksim_program_sample_noisy(ksim_program *p, ksim_noise *n, int64_t B, uint64_t noise_seed,
+                                      uint64_t seed, int32_t rng_mode, uint8_t *out);
+
 /* ---- batch: many programs in one persistent, graph-captured launch ------- */
 
 /* One sampling job of a batch: a component over device rows of f bytes,

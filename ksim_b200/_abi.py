@@ -226,6 +226,14 @@ def _declare(L: ctypes.CDLL) -> None:
         "ksim_batch_launch": (i32, [vp, vp]),
         "ksim_batch_info": (i32, [vp, i64p, ctypes.POINTER(i32), ctypes.POINTER(i32)]),
         "ksim_batch_destroy": (None, [vp]),
+        "ksim_noise_create": (i32, [dp, ctypes.POINTER(i32), i32, _u8p, i32, i32, i32,
+                                    ctypes.POINTER(vp)]),
+        "ksim_noise_destroy": (None, [vp]),
+        "ksim_noise_num_f": (i32, [vp]),
+        "ksim_noise_num_channels": (i32, [vp]),
+        "ksim_noise_sample_device": (i32, [vp, i64, i64, u64, vp, i64, vp]),
+        "ksim_noise_sample": (i32, [vp, i64, i64, u64, _u8p]),
+        "ksim_program_sample_noisy": (i32, [vp, vp, i64, u64, u64, i32, _u8p]),
         "ksim_server_create": (i32, [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]),
         "ksim_server_submit": (i32, [vp, vp, vp, i64, i64, i64, u64, i32, vp, i64p]),
         "ksim_server_wait": (i32, [vp, i64, i32, dp, dp]),

@@ -19,7 +19,7 @@ CSRC = PKG / "csrc"
 LIB = PKG / "lib" / "libksim_b200.so"
 BUILD = PKG / "lib" / "_obj"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["kernels.cu", "api.cu", "peak.cu", "batch.cu", "serve.cu", "noalloc.cu", "image.cpp"]
+SOURCES = ["kernels.cu", "api.cu", "peak.cu", "batch.cu", "serve.cu", "noalloc.cu", "noise.cu", "image.cpp"]
 
 
 def nvcc() -> str:

@@ -573,13 +573,16 @@ namespace {
 // its first row, so the bits equal a single launch over all B shots.
 // packed: f rows of ceil(n_f_cols/8) bytes and output rows of
 // ceil(n_outputs/8) bytes, bit c of a row in byte c/8 at bit c%8.
+// noise (nullable): f rows are drawn on the device from this model with
+// noise_seed instead of being copied from `f`.
 ksim_status program_sample_host(ksim_program *p, const uint8_t *f, int64_t B, int64_t n_f_cols, uint64_t seed,
-                                int32_t rng_mode, uint8_t *out, bool packed)
+                                int32_t rng_mode, uint8_t *out, bool packed, const ksim_noise *noise = nullptr,
+                                uint64_t noise_seed = 0)
 {
     if (!p) return fail(KSIM_ERR_INVALID_ARGUMENT, "program is NULL");
     if (B < 0 || n_f_cols < 0) return fail(KSIM_ERR_INVALID_ARGUMENT, "B and n_f_cols must be >= 0");
     if (B == 0 || p->n_outputs == 0) return check_rng(rng_mode);
-    if ((n_f_cols > 0 && !f) || !out) return fail(KSIM_ERR_INVALID_ARGUMENT, "NULL buffer");
+    if ((n_f_cols > 0 && !f && !noise) || !out) return fail(KSIM_ERR_INVALID_ARGUMENT, "NULL buffer");
     if (check_rng(rng_mode) != KSIM_OK) return KSIM_ERR_INVALID_ARGUMENT;
     if (n_f_cols < p->min_f_cols)
         return fail(KSIM_ERR_INVALID_ARGUMENT, "f_params has " + std::to_string(n_f_cols) +
@@ -618,11 +621,15 @@ ksim_status program_sample_host(ksim_program *p, const uint8_t *f, int64_t B, in
     for (int i = 0; i < n_chunks && e == cudaSuccess && st == KSIM_OK; ++i) {
         const int64_t c0 = (int64_t)i * chunk, n = std::min(chunk, B - c0);
         cudaStream_t cs = (i & 1) ? p->stream_b : p->stream;
-        if (f_row > 0)
-            e = cudaMemcpyAsync(d_in + c0 * f_row, f + c0 * f_row, (size_t)(n * f_row), cudaMemcpyHostToDevice,
-                                p->s_h2d);
-        if (e == cudaSuccess) e = cudaEventRecord(ev_in[i], p->s_h2d);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, ev_in[i], 0);
+        if (noise) {
+            e = launch_noise(noise, n, c0, noise_seed, d_f + c0 * n_f_cols, n_f_cols, cs);
+        } else {
+            if (f_row > 0)
+                e = cudaMemcpyAsync(d_in + c0 * f_row, f + c0 * f_row, (size_t)(n * f_row), cudaMemcpyHostToDevice,
+                                    p->s_h2d);
+            if (e == cudaSuccess) e = cudaEventRecord(ev_in[i], p->s_h2d);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, ev_in[i], 0);
+        }
         if (e == cudaSuccess && packed)
             e = launch_unpack_bits(d_in + c0 * f_row, n, f_row, n_f_cols, d_f + c0 * n_f_cols, cs);
         if (e != cudaSuccess) break;
@@ -667,6 +674,19 @@ ksim_status ksim_program_sample_packed(ksim_program *p, const uint8_t *f_packed,
                                        uint64_t seed, int32_t rng_mode, uint8_t *out_packed)
 {
     return program_sample_host(p, f_packed, B, n_f_cols, seed, rng_mode, out_packed, true);
+}
+
+ksim_status ksim_program_sample_noisy(ksim_program *p, ksim_noise *n, int64_t B, uint64_t noise_seed, uint64_t seed,
+                                      int32_t rng_mode, uint8_t *out)
+{
+    if (!p || !n) return fail(KSIM_ERR_INVALID_ARGUMENT, "program or noise model is NULL");
+    if (noise_device(n) != p->device)
+        return fail(KSIM_ERR_INVALID_ARGUMENT, "program and noise model live on different devices");
+    if (ksim_noise_num_f(n) < p->min_f_cols)
+        return fail(KSIM_ERR_INVALID_ARGUMENT, "the noise model draws " + std::to_string(ksim_noise_num_f(n)) +
+                                                   " f parameters; f_selection needs " +
+                                                   std::to_string(p->min_f_cols));
+    return program_sample_host(p, nullptr, B, ksim_noise_num_f(n), seed, rng_mode, out, false, n, noise_seed);
 }
 
 }  // extern "C"

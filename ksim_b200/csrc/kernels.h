@@ -71,6 +71,12 @@ cudaError_t launch_unpack_bits(const uint8_t *packed, int64_t rows, int64_t pack
 cudaError_t launch_pack_bits(const uint8_t *bytes, int64_t rows, int64_t n_cols, int64_t packed_row,
                              uint8_t *out, cudaStream_t st);
 
+// The noise draw of a noise model (noise.cu): f rows of num_f bytes.
+cudaError_t launch_noise(const ksim_noise *n, int64_t B, int64_t shot_offset, uint64_t seed, uint8_t *f,
+                         int64_t f_stride, cudaStream_t st);
+
+int noise_device(const ksim_noise *n);
+
 // Shared-memory bytes the staged sampler needs for a slot size.
 size_t staged_smem_bytes(int slot_bytes);
 

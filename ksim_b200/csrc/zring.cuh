@@ -598,20 +598,26 @@ KS_HD uint32_t mulhi32(uint32_t a, uint32_t b)
 }
 
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): 10 rounds of the
-// multiply-xor S-box with Weyl key schedule.
-KS_HD double philox_uniform(uint64_t seed, uint64_t shot, uint32_t output)
+// multiply-xor S-box with Weyl key schedule.  c: counter in, block out.
+KS_HD void philox4x32_10(uint32_t (&c)[4], uint64_t seed)
 {
-    uint32_t c0 = (uint32_t)shot, c1 = (uint32_t)(shot >> 32), c2 = output, c3 = 0;
     uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
 #pragma unroll
     for (int r = 0; r < 10; ++r) {
         if (r) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
-        const uint32_t h0 = mulhi32(0xD2511F53u, c0), l0 = 0xD2511F53u * c0;
-        const uint32_t h1 = mulhi32(0xCD9E8D57u, c2), l1 = 0xCD9E8D57u * c2;
-        const uint32_t n0 = h1 ^ c1 ^ k0, n2 = h0 ^ c3 ^ k1;
-        c0 = n0; c1 = l1; c2 = n2; c3 = l0;
+        const uint32_t h0 = mulhi32(0xD2511F53u, c[0]), l0 = 0xD2511F53u * c[0];
+        const uint32_t h1 = mulhi32(0xCD9E8D57u, c[2]), l1 = 0xCD9E8D57u * c[2];
+        const uint32_t n0 = h1 ^ c[1] ^ k0, n2 = h0 ^ c[3] ^ k1;
+        c[0] = n0; c[1] = l1; c[2] = n2; c[3] = l0;
     }
-    const uint64_t bits = ((uint64_t)c1 << 32) | c0;
+}
+
+// Uniform of (shot, output): counter (shot lo, shot hi, output, 0), key = seed.
+KS_HD double philox_uniform(uint64_t seed, uint64_t shot, uint32_t output)
+{
+    uint32_t c[4] = {(uint32_t)shot, (uint32_t)(shot >> 32), output, 0u};
+    philox4x32_10(c, seed);
+    const uint64_t bits = ((uint64_t)c[1] << 32) | c[0];
     return (double)(bits >> 11) * (1.0 / 9007199254740992.0);
 }
 

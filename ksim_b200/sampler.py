@@ -105,4 +105,22 @@ class B200ProgramSampler:
         return out
 
 
+    def sample_noisy(self, noise, shots: int, seed: int, noise_seed: int | None = None,
+                     rng_mode: int = RNG_XORSHIFT, out: np.ndarray | None = None) -> np.ndarray:
+        """Draw f with ``noise`` (a ``DeviceChannelSampler``, shots 0..shots-1 of
+        its stream ``noise_seed``, default its own seed) and sample from it, all
+        on the device; equals ``sample(noise.sample_at(shots, 0), seed)``."""
+        B = int(shots)
+        ns = _as_u64(noise.seed if noise_seed is None else noise_seed)
+        if out is None:
+            out = np.zeros((B, self.num_outputs), np.uint8)
+        elif out.shape != (B, self.num_outputs) or out.dtype != np.uint8 or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous uint8 array of shape {(B, self.num_outputs)}")
+        if B == 0 or self.num_outputs == 0:
+            return out
+        check(self._L.ksim_program_sample_noisy(self._h, noise.handle, B, ns, _as_u64(seed),
+                                                int(rng_mode), _abi.u8ptr(out)))
+        return out
+
+
 KokkosProgramSampler = B200ProgramSampler

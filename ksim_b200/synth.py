@@ -260,6 +260,19 @@ def config(cfg: int, index: int = 0) -> Workload:
     raise ValueError(f"no single-program workload for cfg {cfg}")
 
 
+def noise_model(rng, num_f: int, n_locations: int, p: float = 1e-3, flips_per_bit: int = 2):
+    """A Pauli noise model of the workloads' shape: one single-qubit Pauli
+    channel (X, Y, Z each with probability p) per gate location, its two
+    error bits (x, z) each flipping ``flips_per_bit`` random f parameters.
+    Returns (channel_probs, error_transform) in ChannelSampler's format."""
+    probs = [np.array([1 - 3 * p, p, p, p], np.float64) for _ in range(n_locations)]
+    T = np.zeros((num_f, 2 * n_locations), np.uint8)
+    if num_f:
+        for e in range(2 * n_locations):
+            T[rng.choice(num_f, size=min(flips_per_bit, num_f), replace=False), e] = 1
+    return probs, T
+
+
 def batched_workloads(n_programs: int = 64, seed: int = 3000) -> list:
     """Workload 3: programs with qubits ~U[8,60] (all measured), t ~U[2,16],
     depth 10*qubits, p=1e-3 Pauli noise, shots log-uniform in [1e3, 1e5]."""

@@ -321,3 +321,89 @@ int oracle_max_threads(void)
     return 1;
 #endif
 }
+
+/* ---- noise draw ----------------------------------------------------------
+ * CPU restatement of the device noise draw (ksim_b200/csrc/noise.cu), the
+ * checker for it: per shot, channel c fires iff word c%4 of
+ * Philox(seed, (shot lo, shot hi, c/4, 'NOIS')) < floor(p_fire 2^32); a firing
+ * channel's outcome is the first o whose threshold floor(cdf_o 2^32) exceeds
+ * word 0 of Philox(seed, (shot lo, shot hi, c, 'OUTK')); its f pattern (XOR
+ * of the error_transform columns of the outcome's error bits) is XORed in.
+ * The model follows ChannelSampler._precompute_sparse (compile/channels.py:
+ * 579-622): p_fire = 1 - probs[0], channels with p_fire <= 1e-15 never fire,
+ * conditional CDF cumsum(probs[1:] / p_fire) normalised by its last entry. */
+static uint32_t noise_threshold32(double u)
+{
+    if (!(u > 0.0)) return 0u;
+    double t = floor(ldexp(u, 32));
+    return t >= 4294967295.0 ? 4294967295u : (uint32_t)t;
+}
+
+int oracle_noise_sample(const double *probs, const int32_t *n_bits, int n_channels, const uint8_t *transform,
+                        int num_f, int num_e, int64_t B, int64_t shot_offset, uint64_t seed, uint8_t *out)
+{
+    const uint32_t TAG_FIRE = 0x4E4F4953u, TAG_OUTCOME = 0x4F55544Bu;
+    uint32_t *thr = (uint32_t *)calloc((size_t)(n_channels > 0 ? n_channels : 1), sizeof(uint32_t));
+    int64_t *poff = (int64_t *)calloc((size_t)(n_channels > 0 ? n_channels : 1), sizeof(int64_t));
+    int *eoff = (int *)calloc((size_t)(n_channels > 0 ? n_channels : 1), sizeof(int));
+    int *fires = (int *)calloc((size_t)(n_channels > 0 ? n_channels : 1), sizeof(int));
+    uint32_t **cdf = (uint32_t **)calloc((size_t)(n_channels > 0 ? n_channels : 1), sizeof(uint32_t *));
+    if (!thr || !poff || !eoff || !fires || !cdf) return 1;
+    int64_t po = 0;
+    int eo = 0;
+    for (int i = 0; i < n_channels; ++i) {
+        const int64_t n = (int64_t)1 << n_bits[i];
+        const double *pr = probs + po;
+        poff[i] = po;
+        eoff[i] = eo;
+        po += n;
+        eo += n_bits[i];
+        const double p_fire = 1.0 - pr[0];
+        if (!(p_fire > 1e-15) || n <= 1) continue;
+        fires[i] = 1;
+        thr[i] = noise_threshold32(p_fire);
+        cdf[i] = (uint32_t *)calloc((size_t)n, sizeof(uint32_t));
+        double *cum = (double *)calloc((size_t)n, sizeof(double));
+        double run = 0;
+        for (int64_t o = 1; o < n; ++o) {
+            run += (pr[o] > 0.0 ? pr[o] : 0.0) / p_fire;
+            cum[o - 1] = run;
+        }
+        for (int64_t o = 0; o + 1 < n - 1; ++o) cdf[i][o] = noise_threshold32(cum[o] / cum[n - 2]);
+        free(cum);
+    }
+    /* the device walks the firing channels only, numbered in order */
+    int *idx = (int *)calloc((size_t)(n_channels > 0 ? n_channels : 1), sizeof(int));
+    int n_live = 0;
+    for (int i = 0; i < n_channels; ++i)
+        if (fires[i]) idx[n_live++] = i;
+    uint8_t *f = (uint8_t *)calloc((size_t)(num_f > 0 ? num_f : 1), 1);
+    for (int64_t s = 0; s < B; ++s) {
+        const uint64_t shot = (uint64_t)(shot_offset + s);
+        memset(f, 0, (size_t)(num_f > 0 ? num_f : 1));
+        for (int c = 0; c < n_live; ++c) {
+            uint32_t ctr[4] = {(uint32_t)shot, (uint32_t)(shot >> 32), (uint32_t)(c / 4), TAG_FIRE};
+            uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+            uint32_t x[4];
+            oracle_philox4x32_10(ctr, key, x);
+            const int ch = idx[c];
+            if (x[c % 4] >= thr[ch]) continue;
+            uint32_t ctr2[4] = {(uint32_t)shot, (uint32_t)(shot >> 32), (uint32_t)c, TAG_OUTCOME};
+            uint32_t y[4];
+            oracle_philox4x32_10(ctr2, key, y);
+            const int64_t n_out = ((int64_t)1 << n_bits[ch]) - 1;
+            int64_t o = 0;
+            while (o + 1 < n_out && y[0] >= cdf[ch][o]) ++o;
+            const int64_t outcome = o + 1; /* index into the channel's probs */
+            for (int b = 0; b < n_bits[ch]; ++b) {
+                if (!((outcome >> b) & 1)) continue;
+                const int e = eoff[ch] + b;
+                for (int fi = 0; fi < num_f; ++fi) f[fi] ^= transform[(size_t)fi * num_e + e];
+            }
+        }
+        memcpy(out + s * num_f, f, (size_t)num_f);
+    }
+    for (int i = 0; i < n_channels; ++i) free(cdf[i]);
+    free(cdf); free(thr); free(poff); free(eoff); free(fires); free(idx); free(f);
+    return 0;
+}

@@ -185,3 +185,24 @@ def program_sample(prog, f_params, seed: int, rng_mode: int = 0, oracle_cls=Port
                     [:, :len(comp.graphs) - 1])
     combined = np.concatenate(outs, axis=1) if outs else np.zeros((B, 0), np.uint8)
     return combined[:, np.argsort(prog.output_order)]
+
+
+def noise_sample(channel_probs, error_transform, B: int, shot_offset: int, seed: int) -> np.ndarray:
+    """The device noise draw restated on the CPU (``oracle_noise_sample``):
+    (B, num_f) uint8 for shots shot_offset .. shot_offset + B - 1."""
+    L = _port_lib()
+    f = L.oracle_noise_sample
+    f.restype = ctypes.c_int
+    f.argtypes = [_dp, ctypes.POINTER(ctypes.c_int32), ctypes.c_int, _u8p, ctypes.c_int, ctypes.c_int,
+                  ctypes.c_int64, ctypes.c_int64, ctypes.c_uint64, _u8p]
+    probs = [np.asarray(p, np.float64).reshape(-1) for p in channel_probs]
+    flat = np.ascontiguousarray(np.concatenate(probs) if probs else np.zeros(1))
+    n_bits = np.ascontiguousarray([int(round(np.log2(len(p)))) for p in probs] or [0], np.int32)
+    T = np.ascontiguousarray(np.asarray(error_transform, np.uint8))
+    out = np.zeros((B, T.shape[0]), np.uint8)
+    rc = f(flat.ctypes.data_as(_dp), n_bits.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), len(probs),
+           T.ctypes.data_as(_u8p), T.shape[0], T.shape[1], B, shot_offset, seed & (2**64 - 1),
+           out.ctypes.data_as(_u8p))
+    if rc:
+        raise RuntimeError("oracle noise sample failed")
+    return out
