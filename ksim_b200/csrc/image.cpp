@@ -149,12 +149,15 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
         }
         need_bits = std::max<int64_t>(need_bits, g.P);
     }
-    const int W = supported_words((int)std::max<int64_t>(1, (need_bits + 63) / 64));
-    if (W < 0 || need_bits > 64 * 16) {
+    // one more bit than the parameters: the top bit of the vector is the
+    // constant 1 that folds each column's constant into its parity
+    const int W = supported_words((int)std::max<int64_t>(1, (need_bits + 1 + 63) / 64));
+    if (W < 0 || need_bits + 1 > 64 * 16) {
         err = "parameter vector of " + std::to_string(need_bits) +
-              " bits exceeds the 1024 this build supports";
+              " bits exceeds the 1023 this build supports";
         return KSIM_ERR_UNSUPPORTED;
     }
+    const uint64_t one_bit = 1ull << 63;  // in word W - 1
     const int R1 = rec1_words(W), R2 = rec2_words(W);
 
     img = HostImage();
@@ -227,18 +230,53 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 Lmax = std::max(Lmax, transient);
                 if (transient > kLim) unsafe = true;
             };
-            // NodePhases
-            uint32_t nu = 0;
-            int n_np = 0;
+            // NodePhases.  A column's mask carries the constant bit iff bit 2
+            // of its phase is set, so its parity is the sign of w^(4 par):
+            // factor = 1 + (-1)^parity w^(phase & 3).  Every factor has
+            // valuation <= 2 and the reference halves at most once per
+            // factor, so the block's result is order-independent:
+            // prod / 2^floor(sum nu / 4).  Fast terms therefore run their
+            // columns grouped by rotation class (j = 0, 2, 1, 3), one
+            // branch-free loop per class; exact terms keep the reference's
+            // order.  The halving steps and the bound follow the run order.
+            struct NpCol { uint32_t phase; std::vector<uint64_t> m; };
+            std::vector<NpCol> npc((size_t)cnp);
             for (int c = 0; c < cnp; ++c) {
                 const size_t ci = (size_t)t * g.Tnp + c;
                 if (!pack_mask(g.np_params + ci * P, P, W, mask.data())) {
                     err = gname + ": np_params holds a byte other than 0/1";
                     return KSIM_ERR_MALFORMED_PROGRAM;
                 }
-                const uint32_t phase = g.np_phases[ci] & 7u;
-                const uint32_t j = phase & 3u;
-                uint32_t red = 0;
+                npc[c].phase = g.np_phases[ci] & 7u;
+                npc[c].m.assign(mask.begin(), mask.begin() + W);
+                if (npc[c].phase & 4u) npc[c].m[W - 1] |= one_bit;
+            }
+            static const int kClassRank[4] = {0, 2, 1, 3};  // j = 0, 1, 2, 3 -> run position
+            std::vector<int> order((size_t)cnp);
+            for (int c = 0; c < cnp; ++c) order[c] = c;
+            std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+                return kClassRank[npc[a].phase & 3u] < kClassRank[npc[b].phase & 3u];
+            });
+            int n_cls[4] = {0, 0, 0, 0};
+            for (int c = 0; c < cnp; ++c) ++n_cls[npc[c].phase & 3u];
+            // A term whose factor 2 / 0 column yields 0 keeps the pw the
+            // reference had at that column: its surviving earlier factor-2
+            // columns (counted at run time, they run first in their original
+            // relative order) plus the halvings before the column in the
+            // reference's order, stored in the column word.
+            std::vector<uint32_t> h_before((size_t)cnp, 0);
+            {
+                uint32_t cum = 0;
+                for (int c = 0; c < cnp; ++c) {
+                    const uint32_t j = npc[c].phase & 3u;
+                    h_before[c] = cum / 4;
+                    if (j) cum += (j & 1u) ? 1u : 2u;
+                }
+            }
+            std::vector<uint32_t> np_red((size_t)cnp, 0);  // halving flag, by run position
+            uint32_t nu = 0;
+            for (int r = 0; r < cnp; ++r) {
+                const uint32_t j = npc[order[r]].phase & 3u;
                 if (j == 0) {
                     step(L + 1.0);  // 2z before it is halved back
                 } else {
@@ -247,15 +285,12 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                     step(L);
                     if (nu >= 4) {
                         nu -= 4;
-                        red = 1;
+                        np_red[r] = 1;
                         L -= 1.0;
                     }
                 }
-                for (int w = 0; w < W; ++w) put64(rec, mask[w]);
-                put64(rec, phase | (red ? NP_REDUCE_BIT : 0u));
-                for (int w = W + 1; w < R1; ++w) put64(rec, 0);
-                ++n_np;
             }
+            const int n_np = cnp;
             // HalfPi
             int n_hp = 0;
             for (int c = 0; c < g.Thp; ++c) {
@@ -284,6 +319,9 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 const bool psi0 = pc == 0 && all_zero(mask.data(), W);
                 const bool phi0 = qc == 0 && all_zero(mask.data() + W, W);
                 if (psi0 || phi0) continue;
+                // constants folded into the parities: psi = parity(psi mask), phi likewise
+                if (pc) mask[W - 1] |= one_bit;
+                if (qc) mask[2 * W - 1] |= one_bit;
                 for (int w = 0; w < 2 * W; ++w) put64(rec, mask[w]);
                 put64(rec, pc | (qc << 1));
                 for (int w = 2 * W + 1; w < R2; ++w) put64(rec, 0);
@@ -298,13 +336,21 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                     err = gname + ": ph params hold a byte other than 0/1";
                     return KSIM_ERR_MALFORMED_PROGRAM;
                 }
-                const uint32_t ac = g.ph_alpha[ci] & 7u, bc = g.ph_beta[ci] & 7u;
-                uint64_t cw = ac | (bc << 3);
+                const uint32_t ac = g.ph_alpha[ci] & 7u, bc = g.ph_beta[ci] & 7u, gc = (ac + bc) & 7u;
+                const uint32_t a2 = ac >> 2, b2 = bc >> 2;
+                // the masks carry bit 2 of alpha / beta in the constant bit, so
+                // pa' = pa ^ a2 and pb' = pb ^ b2 are the signs of the w^a and
+                // w^b copies; the -w^(a+b) copy's sign is K ^ pa' ^ pb'
+                if (a2) mask[W - 1] |= one_bit;
+                if (b2) mask[2 * W - 1] |= one_bit;
+                const uint32_t K = ((gc >> 2) ^ 1u ^ a2 ^ b2) & 1u;
+                uint64_t cw = (ac & 3u) | (K << 2) | ((bc & 3u) << 3) | ((gc & 3u) << 5);
                 double fmax = 0;
-                for (uint32_t combo = 0; combo < 4; ++combo) {
+                for (uint32_t combo = 0; combo < 4; ++combo) {  // combo = raw pa | pb << 1
                     int64_t f[4];
                     phase_pair((int)(ac ^ ((combo & 1u) << 2)), (int)(bc ^ ((combo >> 1) << 2)), f);
-                    cw |= (uint64_t)zw_valuation(f) << (8 + 4 * combo);
+                    const uint32_t folded = combo ^ (a2 | (b2 << 1));  // index pa' | pb' << 1
+                    cw |= (uint64_t)zw_valuation(f) << (8 + 4 * folded);
                     fmax = std::max(fmax, max_embed(f));
                 }
                 step(L + 2.0);  // partial sums of four rotated copies
@@ -328,12 +374,26 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             // every value the fast path must know exactly is below 2^Lmax; with
             // Lmax <= 30.5 it fits int32 and the term runs on 32-bit words
             uint32_t flags = unsafe ? TF_SLOW : (Lmax <= 30.5 ? TF_NARROW : 0u);
+            // NodePhases records: class order with halving flags for the fast
+            // paths, the reference's order for the exact path
+            std::vector<uint8_t> np_rec;
+            for (int r = 0; r < cnp; ++r) {
+                const int c = unsafe ? r : order[r];
+                for (int w = 0; w < W; ++w) put64(np_rec, npc[c].m[w]);
+                put64(np_rec, (uint64_t)npc[c].phase | ((!unsafe && np_red[r]) ? NP_REDUCE_BIT : 0u) |
+                                  ((uint64_t)std::min<uint32_t>(h_before[c], 0xFFFFu) << 16));
+                for (int w = W + 1; w < R1; ++w) put64(np_rec, 0);
+            }
             if (g.pf_has_approx) flags |= TF_APX;
             put32(out, (uint32_t)n_np | ((uint32_t)n_hp << 16));
             put32(out, (uint32_t)n_pp | ((uint32_t)n_ph << 16));
             put32(out, (g.pf_phase_idx[t] & 7u) | (nu << 8) | (flags << 16));
             put32(out, (uint32_t)g.pf_power2[t]);
             for (int i = 0; i < 4; ++i) put32(out, (uint32_t)ff[i]);
+            // NodePhases run lengths per rotation class, in run order (j = 0, 2, 1, 3)
+            put32(out, (uint32_t)n_cls[0] | ((uint32_t)n_cls[2] << 16));
+            put32(out, (uint32_t)n_cls[1] | ((uint32_t)n_cls[3] << 16));
+            put64(out, 0);
             if (g.pf_has_approx) {
                 double ar = g.pf_approx_f32[2 * (size_t)t], ai = g.pf_approx_f32[2 * (size_t)t + 1];
                 uint64_t u;
@@ -342,6 +402,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 std::memcpy(&u, &ai, 8);
                 put64(out, u);
             }
+            out.insert(out.end(), np_rec.begin(), np_rec.end());
             out.insert(out.end(), rec.begin(), rec.end());
             (void)ff64;
             const int64_t tb = (int64_t)out.size() - start;

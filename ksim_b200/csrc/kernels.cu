@@ -44,6 +44,7 @@ __global__ void __launch_bounds__(128) k_eval(const EvalJob j)
         for (int b = 0; b < lim; ++b) x |= (uint64_t)(row[64 * w + b] & 1u) << b;
         v[w] = x;
     }
+    set_one_bit<W>(v);
     const GraphDir gd = j.gdir[j.graph];
     const uint8_t *p = j.image + gd.stream_off;
     uint32_t risk = 0;

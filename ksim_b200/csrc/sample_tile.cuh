@@ -141,7 +141,7 @@ __device__ __forceinline__ uint32_t get_bit(const uint64_t (&v)[W], int pos)
 
 // Parameter vector of graph k: [f | m_0..m_{nm-1}] and, for k >= 1, the
 // "trying" bit on every position from F+nm up to the graph's P
-// (kokkos_sim.cpp:10-14 / zx_eval.hpp:86-90).
+// (kokkos_sim.cpp:10-14 / zx_eval.hpp:86-90), plus the constant-one top bit.
 template <int W>
 __device__ __forceinline__ void graph_vector(uint64_t (&vk)[W], const uint64_t (&v)[W], int F, int k, int P)
 {
@@ -149,6 +149,7 @@ __device__ __forceinline__ void graph_vector(uint64_t (&vk)[W], const uint64_t (
     const int64_t lo = (int64_t)F + nm;
 #pragma unroll
     for (int w = 0; w < W; ++w) vk[w] = (v[w] & bit_range(w, 0, lo)) | (k > 0 ? bit_range(w, lo, P) : 0ull);
+    set_one_bit<W>(vk);
 }
 
 // Issue the copy of chunk c of job j; gidx is its position in the CTA's

@@ -44,7 +44,7 @@ namespace ksim {
 // TF_NARROW: every value the fast path must know exactly (at each halving
 // and at the end) is proven below 2^31, so it runs on 32-bit coefficients.
 enum : uint32_t { TF_SLOW = 1u, TF_APX = 2u, TF_NARROW = 4u };
-constexpr int TERM_HDR_BYTES = 32;
+constexpr int TERM_HDR_BYTES = 48;
 constexpr int TERM_APX_BYTES = 16;
 // NodePhases / HalfPi column: W mask words + 1 constant word, padded to 16 B
 KS_HD constexpr int rec1_words(int W) { return (W + 2) & ~1; }
@@ -222,7 +222,16 @@ struct TermHdr {
     uint32_t pf_idx, nu_np, flags;
     int32_t power2;
     Zu ff;
+    uint32_t n_cls[4];  // NodePhases run lengths in run order: j = 0, 2, 1, 3
 };
+
+// The parameter vector's top bit (bit 63 of word W-1) is the constant 1; a
+// column mask that includes it has its constant folded into its parity.
+template <int W>
+KS_HD void set_one_bit(uint64_t (&v)[W])
+{
+    v[W - 1] |= 1ull << 63;
+}
 
 KS_HD TermHdr load_hdr(const uint8_t *p)
 {
@@ -236,6 +245,9 @@ KS_HD TermHdr load_hdr(const uint8_t *p)
     const int32_t *ff = (const int32_t *)(p + 16);
     h.ff.a = (uint64_t)(int64_t)ff[0]; h.ff.b = (uint64_t)(int64_t)ff[1];
     h.ff.c = (uint64_t)(int64_t)ff[2]; h.ff.d = (uint64_t)(int64_t)ff[3];
+    const uint32_t c0 = u[8], c1 = u[9];
+    h.n_cls[0] = c0 & 0xFFFFu; h.n_cls[1] = c0 >> 16;
+    h.n_cls[2] = c1 & 0xFFFFu; h.n_cls[3] = c1 >> 16;
     return h;
 }
 
@@ -269,6 +281,52 @@ struct TermOut {
     uint32_t risk;  // KSIM_FLAG_INT64_RISK raised by the exact path
 };
 
+// A run of NodePhases columns of rotation class J, for S shots: factor
+// 1 + (-1)^parity w^J (the mask carries the phase's bit 2 in the constant
+// bit), i.e. z += +-R_J(z); J = 0 is the factor 2 (halved straight back,
+// pw + 1) or 0 (the term dies).  Halvings where the host marked them.
+template <int W, typename T, int S, int J>
+KS_HD const uint64_t *np_class(const uint64_t *q, uint32_t n, const uint64_t (&v)[S][W], Zr<T> (&z)[S],
+                               int64_t (&pw)[S], uint32_t (&alive)[S])
+{
+    constexpr int R1 = rec1_words(W);
+    for (uint32_t t = 0; t < n; ++t, q += R1) {
+        uint64_t r[R1];
+        load_rec<R1>(q, r);
+        uint64_t mw[W];
+#pragma unroll
+        for (int w = 0; w < W; ++w) mw[w] = r[w];
+        uint32_t neg[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) neg[s] = parity<W>(mw, v[s]);
+        if (J == 0) {
+            // a zero factor freezes pw at the reference's value at this column
+            const int64_t h_before = (int64_t)(((uint32_t)r[W] >> 16) & 0xFFFFu);
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                pw[s] += (alive[s] & (neg[s] ^ 1u)) + (int64_t)(alive[s] & neg[s]) * h_before;
+                alive[s] &= neg[s] ^ 1u;
+                const T keep = (T)0 - (T)alive[s];
+                z[s].a &= keep; z[s].b &= keep; z[s].c &= keep; z[s].d &= keep;
+            }
+        } else {
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const Zr<T> t0 = z[s];
+                add_rot(z[s], t0, (uint32_t)J, (T)0 - (T)neg[s]);
+            }
+            if ((uint32_t)r[W] & NP_REDUCE_BIT) {
+#pragma unroll
+                for (int s = 0; s < S; ++s) {
+                    shr_all(z[s], 1u);
+                    pw[s] += alive[s];
+                }
+            }
+        }
+    }
+    return q;
+}
+
 // Fast path: exact when the host proved every coefficient stays below 2^62
 // (T = uint64_t) or that every value it must know exactly stays below 2^31
 // (T = uint32_t, TF_NARROW): adds and multiplies wrap, so intermediate sums
@@ -291,42 +349,12 @@ KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const ui
         alive[s] = 1;
     }
 
-    // NodePhases
-    for (uint32_t t = 0; t < h.n_np; ++t, q += R1) {
-        uint64_t r[R1];
-        load_rec<R1>(q, r);
-        uint64_t mw[W];
-#pragma unroll
-        for (int w = 0; w < W; ++w) mw[w] = r[w];
-        const uint32_t cw = (uint32_t)r[W];
-        const uint32_t j = cw & 3u, c2 = (cw >> 2) & 1u;
-        uint32_t neg[S];
-#pragma unroll
-        for (int s = 0; s < S; ++s) neg[s] = parity<W>(mw, v[s]) ^ c2;
-        if (j == 0) {
-            // factor 2 (halved straight back, pw + 1) or 0 (the term dies)
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-                pw[s] += alive[s] & (neg[s] ^ 1u);
-                alive[s] &= neg[s] ^ 1u;
-                const T keep = (T)0 - (T)alive[s];
-                z[s].a &= keep; z[s].b &= keep; z[s].c &= keep; z[s].d &= keep;
-            }
-        } else {
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-                const Zr<T> t0 = z[s];
-                add_rot(z[s], t0, j, (T)0 - (T)neg[s]);
-            }
-            if (cw & NP_REDUCE_BIT) {
-#pragma unroll
-                for (int s = 0; s < S; ++s) {
-                    shr_all(z[s], 1u);
-                    pw[s] += alive[s];
-                }
-            }
-        }
-    }
+    // NodePhases: one branch-free loop per rotation class, in the run order
+    // the host packed (j = 0, 2, 1, 3)
+    q = np_class<W, T, S, 0>(q, h.n_cls[0], v, z, pw, alive);
+    q = np_class<W, T, S, 2>(q, h.n_cls[1], v, z, pw, alive);
+    q = np_class<W, T, S, 1>(q, h.n_cls[2], v, z, pw, alive);
+    q = np_class<W, T, S, 3>(q, h.n_cls[3], v, z, pw, alive);
     // HalfPi: w^(sum par*coeff); its renormalisation cannot fire (nu < 4 here)
     {
         uint32_t tot[S];
@@ -356,13 +384,8 @@ KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const ui
             uint64_t ma[W], mb[W];
 #pragma unroll
             for (int w = 0; w < W; ++w) { ma[w] = r[w]; mb[w] = r[W + w]; }
-            const uint32_t cw = (uint32_t)r[2 * W];
 #pragma unroll
-            for (int s = 0; s < S; ++s) {
-                const uint32_t psi = (cw ^ parity<W>(ma, v[s])) & 1u;
-                const uint32_t phi = ((cw >> 1) ^ parity<W>(mb, v[s])) & 1u;
-                e[s] ^= psi & phi;
-            }
+            for (int s = 0; s < S; ++s) e[s] ^= parity<W>(ma, v[s]) & parity<W>(mb, v[s]);
         }
 #pragma unroll
         for (int s = 0; s < S; ++s) {
@@ -382,14 +405,15 @@ KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const ui
 #pragma unroll
             for (int w = 0; w < W; ++w) { ma[w] = r[w]; mb[w] = r[W + w]; }
             const uint32_t cw = (uint32_t)r[2 * W];
-            const uint32_t ac = cw & 7u, bc = (cw >> 3) & 7u, gc = (ac + bc) & 7u;
+            const uint32_t ja = cw & 3u, K = (cw >> 2) & 1u, jb = (cw >> 3) & 3u, jg = (cw >> 5) & 3u;
 #pragma unroll
             for (int s = 0; s < S; ++s) {
+                // pa, pb: parities with bit 2 of alpha / beta folded in
                 const uint32_t pa = parity<W>(ma, v[s]), pb = parity<W>(mb, v[s]);
                 const Zr<T> t0 = z[s];
-                add_rot(z[s], t0, ac & 3u, (T)0 - (T)(((ac >> 2) ^ pa) & 1u));
-                add_rot(z[s], t0, bc & 3u, (T)0 - (T)(((bc >> 2) ^ pb) & 1u));
-                add_rot(z[s], t0, gc & 3u, (T)0 - (T)(((gc >> 2) ^ pa ^ pb ^ 1u) & 1u));
+                add_rot(z[s], t0, ja, (T)0 - (T)pa);
+                add_rot(z[s], t0, jb, (T)0 - (T)pb);
+                add_rot(z[s], t0, jg, (T)0 - (T)(K ^ pa ^ pb));
                 const uint32_t nf = (cw >> (8 + 4 * (pa | (pb << 1)))) & 15u;
                 alive[s] &= (nf != NU_ZERO) ? 1u : 0u;
                 nu[s] += nf;
@@ -432,8 +456,10 @@ KS_HD const uint8_t *eval_term_exact(const uint8_t *p, const TermHdr &h, const u
     int64_t pw = 0;
     uint32_t risk = 0;
     for (uint32_t t = 0; t < h.n_np; ++t, q += R1) {
+        // phase + 4 par (mod 8) = (phase & 3) + 4 (par ^ phase bit 2): the mask
+        // carries bit 2 of the phase in the constant bit
         const uint32_t cw = (uint32_t)q[W];
-        const uint32_t k = ((parity<W>(q, v) << 2) + (cw & 7u)) & 7u;
+        const uint32_t k = ((parity<W>(q, v) << 2) | (cw & 3u)) & 7u;
         Zu u = rot_var(one, k);
         u.a += 1;
         risk |= over62(z);
@@ -451,17 +477,15 @@ KS_HD const uint8_t *eval_term_exact(const uint8_t *p, const TermHdr &h, const u
     {
         uint32_t e = 0;
         for (uint32_t t = 0; t < h.n_pp; ++t, q += R2) {
-            const uint32_t cw = (uint32_t)q[2 * W];
-            const uint32_t psi = (cw + parity<W>(q, v)) & 1u;
-            const uint32_t phi = ((cw >> 1) + parity<W>(q + W, v)) & 1u;
+            const uint32_t psi = parity<W>(q, v), phi = parity<W>(q + W, v);  // constants folded in
             e ^= psi & phi;
         }
         if (e) { z.a = 0 - z.a; z.b = 0 - z.b; z.c = 0 - z.c; z.d = 0 - z.d; }
     }
     for (uint32_t t = 0; t < h.n_ph; ++t, q += R2) {
         const uint32_t cw = (uint32_t)q[2 * W];
-        const uint32_t al = ((cw & 7u) + 4u * parity<W>(q, v)) & 7u;
-        const uint32_t be = (((cw >> 3) & 7u) + 4u * parity<W>(q + W, v)) & 7u;
+        const uint32_t al = ((cw & 3u) | (parity<W>(q, v) << 2)) & 7u;
+        const uint32_t be = (((cw >> 3) & 3u) | (parity<W>(q + W, v) << 2)) & 7u;
         const Zu u = rot_var(one, al), x = rot_var(one, be), y = rot_var(one, (al + be) & 7u);
         Zu term = {1 + u.a + x.a - y.a, u.b + x.b - y.b, u.c + x.c - y.c, u.d + x.d - y.d};
         risk |= over62(z);

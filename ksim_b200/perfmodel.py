@@ -70,7 +70,7 @@ def words_for(comp) -> int:
     supported = (1, 2, 3, 4, 5, 6, 8, 10, 12, 16)
     F = int(np.asarray(comp.f_selection).shape[0])
     bits = max([F + len(comp.graphs) - 1] + [int(g.np_params.shape[2]) for g in comp.graphs] + [1])
-    need = (bits + 63) // 64
+    need = (bits + 1 + 63) // 64  # plus the constant-one bit
     return next(w for w in supported if w >= need)
 
 

@@ -25,6 +25,7 @@ void pack_row(const uint8_t *row, int64_t n, uint64_t (&v)[W])
 {
     for (int w = 0; w < W; ++w) v[w] = 0;
     for (int64_t c = 0; c < n && c < 64 * W; ++c) v[c >> 6] |= (uint64_t)(row[c] & 1u) << (c & 63);
+    set_one_bit<W>(v);
 }
 
 // Modes 3 (per-term numerators) and 4 (complex amplitude): the same as 2 and
@@ -117,6 +118,7 @@ void sample_rows(const HostImage &img, const uint8_t *f, int64_t B, uint64_t see
             uint64_t vk[W];
             for (int w = 0; w < W; ++w)
                 vk[w] = (v[w] & bit_range(w, 0, F + nm)) | (k > 0 ? bit_range(w, F + nm, img.gdir[k].P) : 0);
+            set_one_bit<W>(vk);
             double re = 0, im = 0;
             uint32_t risk = 0;
             eval_terms<W>(img.bytes.data() + img.gdir[k].stream_off, (uint32_t)img.gdir[k].G, vk, re, im, risk);
