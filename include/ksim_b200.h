@@ -371,6 +371,15 @@ void ksim_server_destroy(ksim_server *s);
 
 /* ---- measurement --------------------------------------------------------- */
 
+/* The roofline numerator: int32 operations one shot costs on a component in
+ * the formulation the kernels run (32-bit words for terms proven below 2^31,
+ * 64-bit words otherwise, the reference's step-by-step arithmetic for terms
+ * on the exact path), and how many terms take each path (paths[0] 32-bit,
+ * paths[1] 64-bit, paths[2] exact; nullable).  Host only: no device is
+ * needed.  No reference counterpart. */
+ksim_status ksim_work_model(const ksim_graph_desc *graphs, int32_t n_graphs, int32_t num_f,
+                            double *ops_per_shot, int64_t *paths);
+
 /* Integer-pipe throughput of this GPU for the sampler's instruction mix
  * (32-bit add / shift / logic), in int32 lane-operations per second: the
  * roofline denominator of the sampling kernels.  No reference counterpart. */

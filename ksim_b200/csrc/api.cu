@@ -124,6 +124,23 @@ int32_t ksim_device_count(void)
     return n;
 }
 
+ksim_status ksim_work_model(const ksim_graph_desc *graphs, int32_t n_graphs, int32_t num_f, double *ops_per_shot,
+                            int64_t *paths)
+{
+    if (!ops_per_shot) return fail(KSIM_ERR_INVALID_ARGUMENT, "ops_per_shot is NULL");
+    HostImage img;
+    std::string err;
+    int st = build_image(graphs, n_graphs, num_f, img, err);
+    if (st != KSIM_OK) return fail((ksim_status)st, err);
+    *ops_per_shot = img.work_ops;
+    if (paths) {
+        paths[0] = img.n_narrow_terms;
+        paths[1] = img.n_terms - img.n_narrow_terms - img.n_slow_terms;
+        paths[2] = img.n_slow_terms;
+    }
+    return KSIM_OK;
+}
+
 ksim_status ksim_component_create(const ksim_graph_desc *graphs, int32_t n_graphs, int32_t num_f,
                                   int32_t device, ksim_component **out)
 {

@@ -99,6 +99,37 @@ bool all_zero(const uint64_t *m, int W)
 
 }  // namespace
 
+// Work model: int32 operations one shot costs for one term / graph in the
+// formulation the kernels run (the roofline numerator).  c = 1 on 32-bit
+// words (TF_NARROW), 2 on 64-bit words; exact-path terms are costed as the
+// reference's step-by-step arithmetic (one Z[w] product = 16 64-bit
+// multiplies x 3 + 12 64-bit adds x 2 + renormalisation 12 = 84 per factor).
+//   parity of one W-word mask: 3W (and / xor / fold) + 2 (popcount, bit)
+//   NodePhases j != 0: parity + 1 (sign) + 4c (signed adds) [+ 4c + 1 halving]
+//   NodePhases j == 0: parity + 2
+//   HalfPi: parity + 1;  PiProducts: 2 parities + 1
+//   PhasePairs: 2 parities + 3 (signs) + 12c (three rotated adds)
+//               + 4 (valuation) + 4c + 1 (conditional halving)
+//   per term: rotations and signs 28c, floatfactor product 28 (c = 1) or
+//             72 (c = 2), renormalisation 6c, complex value and sum 16
+//   per graph: parameter vector 4W + 8, Bernoulli step 10
+double term_work(int W, uint32_t flags, const int n_cls[4], int n_hp, int n_pp, int n_ph, int n_halvings)
+{
+    const double par = 3.0 * W + 2.0;
+    const int n_np = n_cls[0] + n_cls[1] + n_cls[2] + n_cls[3];
+    if (flags & TF_SLOW)
+        return 84.0 * (n_np + n_ph + 3) + par * (n_np + n_hp + 2.0 * n_pp + 2.0 * n_ph) + 16.0;
+    const double c = (flags & TF_NARROW) ? 1.0 : 2.0;
+    double w = n_cls[0] * (par + 2.0);
+    w += (n_np - n_cls[0]) * (par + 1.0 + 4.0 * c) + n_halvings * (4.0 * c + 1.0);
+    w += n_hp * (par + 1.0) + n_pp * (2.0 * par + 1.0);
+    w += n_ph * (2.0 * par + 3.0 + 12.0 * c + 4.0 + 4.0 * c + 1.0);
+    w += 28.0 * c + (c == 1.0 ? 28.0 : 72.0) + 6.0 * c + 16.0;
+    return w;
+}
+
+double graph_work(int W) { return 4.0 * W + 8.0 + 10.0; }
+
 int supported_words(int needed)
 {
     for (int w : kWords)
@@ -411,8 +442,11 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             img.n_slow_terms += unsafe ? 1 : 0;
             img.n_narrow_terms += (flags & TF_NARROW) ? 1 : 0;
             img.n_columns += n_np + n_hp + n_pp + n_ph;
+            img.work_ops += term_work(W, flags, n_cls, n_hp, n_pp, n_ph,
+                                      (int)std::count(np_red.begin(), np_red.end(), 1u));
         }
         toff.push_back((int64_t)out.size());
+        img.work_ops += graph_work(W);
         gd.stream_bytes = (int64_t)out.size() - gd.stream_off;
         gd.n_chunks = 0;
         gd.first_chunk = 0;

@@ -35,6 +35,7 @@ struct HostImage {
     std::vector<std::vector<int64_t>> term_off;  // per graph: term start offsets + end
     int64_t max_term_bytes = 0;
     int64_t n_terms = 0, n_slow_terms = 0, n_narrow_terms = 0;
+    double work_ops = 0;  // int32 operations per shot, all graphs (term_work / graph_work)
     int64_t n_columns = 0;
 };
 
@@ -42,6 +43,11 @@ struct HostImage {
 // `err` says which graph / array is wrong.
 int build_image(const ksim_graph_desc *graphs, int n_graphs, int F, HostImage &out,
                 std::string &err);
+
+// int32 operations of one shot for one term / one graph (the roofline
+// numerator; see image.cpp).
+double term_work(int W, uint32_t flags, const int n_cls[4], int n_hp, int n_pp, int n_ph, int n_halvings);
+double graph_work(int W);
 
 // Split every graph's term stream into chunks of whole terms of at most
 // slot_bytes (an empty graph gets one empty chunk).  Returns false if a single

@@ -281,6 +281,26 @@ struct TermOut {
     uint32_t risk;  // KSIM_FLAG_INT64_RISK raised by the exact path
 };
 
+// One PhasePairs factor 1 + sa w^JA + sb w^JB + sg w^(JA+JB) applied to z,
+// sa = (-1)^pa, sb = (-1)^pb, sg = -(-1)^(K ^ pa ^ pb) (bit 2 of alpha / beta
+// folded into pa / pb; K carries the rest of the -w^(alpha+beta) sign).
+template <typename T, int JA, int JB>
+KS_HD void ph_update(Zr<T> &z, uint32_t pa, uint32_t pb, uint32_t K)
+{
+    constexpr uint32_t JG = (uint32_t)((JA + JB) & 3);
+    const T ma = (T)0 - (T)pa, mb = (T)0 - (T)pb, mg = (T)0 - (T)(K ^ pa ^ pb);
+    const Zr<T> t0 = z;
+    if constexpr (JA == 0 && JB == 0) {
+        // a scalar factor 1 + sa + sb + sg
+        const T f = (T)1 + ((T)1 ^ (ma & (T)~(T)1)) + ((T)1 ^ (mb & (T)~(T)1)) + ((T)1 ^ (mg & (T)~(T)1));
+        z.a = t0.a * f; z.b = t0.b * f; z.c = t0.c * f; z.d = t0.d * f;
+    } else {
+        add_rot(z, t0, (uint32_t)JA, ma);
+        add_rot(z, t0, (uint32_t)JB, mb);
+        add_rot(z, t0, JG, mg);
+    }
+}
+
 // A run of NodePhases columns of rotation class J, for S shots: factor
 // 1 + (-1)^parity w^J (the mask carries the phase's bit 2 in the constant
 // bit), i.e. z += +-R_J(z); J = 0 is the factor 2 (halved straight back,
@@ -405,16 +425,29 @@ KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const ui
 #pragma unroll
             for (int w = 0; w < W; ++w) { ma[w] = r[w]; mb[w] = r[W + w]; }
             const uint32_t cw = (uint32_t)r[2 * W];
-            const uint32_t ja = cw & 3u, K = (cw >> 2) & 1u, jb = (cw >> 3) & 3u, jg = (cw >> 5) & 3u;
+            const uint32_t K = (cw >> 2) & 1u;
+            // pa, pb: parities with bit 2 of alpha / beta folded in
+            uint32_t pa[S], pb[S];
 #pragma unroll
             for (int s = 0; s < S; ++s) {
-                // pa, pb: parities with bit 2 of alpha / beta folded in
-                const uint32_t pa = parity<W>(ma, v[s]), pb = parity<W>(mb, v[s]);
-                const Zr<T> t0 = z[s];
-                add_rot(z[s], t0, ja, (T)0 - (T)pa);
-                add_rot(z[s], t0, jb, (T)0 - (T)pb);
-                add_rot(z[s], t0, jg, (T)0 - (T)(K ^ pa ^ pb));
-                const uint32_t nf = (cw >> (8 + 4 * (pa | (pb << 1)))) & 15u;
+                pa[s] = parity<W>(ma, v[s]);
+                pb[s] = parity<W>(mb, v[s]);
+            }
+            // one branch on the rotation pair; the third rotation is their sum
+            switch ((cw & 3u) | ((cw >> 1) & 12u)) {
+#define KSIM_PH_CASE(JA, JB)                                                        \
+    case (JA) | ((JB) << 2):                                                        \
+        _Pragma("unroll") for (int s = 0; s < S; ++s) ph_update<T, JA, JB>(z[s], pa[s], pb[s], K); \
+        break;
+            KSIM_PH_CASE(0, 0) KSIM_PH_CASE(1, 0) KSIM_PH_CASE(2, 0) KSIM_PH_CASE(3, 0)
+            KSIM_PH_CASE(0, 1) KSIM_PH_CASE(1, 1) KSIM_PH_CASE(2, 1) KSIM_PH_CASE(3, 1)
+            KSIM_PH_CASE(0, 2) KSIM_PH_CASE(1, 2) KSIM_PH_CASE(2, 2) KSIM_PH_CASE(3, 2)
+            KSIM_PH_CASE(0, 3) KSIM_PH_CASE(1, 3) KSIM_PH_CASE(2, 3) KSIM_PH_CASE(3, 3)
+#undef KSIM_PH_CASE
+            }
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const uint32_t nf = (cw >> (8 + 4 * (pa[s] | (pb[s] << 1)))) & 15u;
                 alive[s] &= (nf != NU_ZERO) ? 1u : 0u;
                 nu[s] += nf;
                 const uint32_t red = alive[s] & (nu[s] >= 4 ? 1u : 0u);
