@@ -322,6 +322,44 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 }
             }
             const int n_np = cnp;
+            // Halvings inside a class run are periodic (every 4 columns for
+            // j odd, nu = 1; every 2 for j = 2, nu = 2) once the first has
+            // happened, so each class is encoded as head columns (then a
+            // halving), k groups of 4 / nu columns (each followed by a
+            // halving) and tail columns: word = k | head << 16 | tail << 20.
+            // j = 0 columns never halve: word = their count.
+            uint32_t np_sched[4] = {0, 0, 0, 0};
+            {
+                static const uint32_t kRunClass[4] = {0, 2, 1, 3};
+                int r0 = 0;
+                for (int ci = 0; ci < 4; ++ci) {
+                    const uint32_t j = kRunClass[ci];
+                    const int n = n_cls[j];
+                    if (j == 0) {
+                        np_sched[ci] = (uint32_t)n;
+                        r0 += n;
+                        continue;
+                    }
+                    const int grp = (j & 1u) ? 4 : 2;
+                    std::vector<int> hv;  // halving positions within the class
+                    for (int i = 0; i < n; ++i)
+                        if (np_red[r0 + i]) hv.push_back(i);
+                    int head = 0, k = 0, tail = n;
+                    if (!hv.empty()) {
+                        head = hv[0] + 1;
+                        k = (int)hv.size() - 1;
+                        tail = n - head - k * grp;
+                        for (int h = 1; h < (int)hv.size(); ++h)
+                            if (hv[h] != hv[0] + h * grp) tail = -1;
+                    }
+                    if (head > grp || tail < 0 || tail >= grp + (hv.empty() ? 0 : 0) || k > 0xFFFF) {
+                        err = gname + ": internal error: NodePhases halving schedule is not periodic";
+                        return KSIM_ERR_INTERNAL;
+                    }
+                    np_sched[ci] = (uint32_t)k | ((uint32_t)head << 16) | ((uint32_t)tail << 20);
+                    r0 += n;
+                }
+            }
             // HalfPi
             int n_hp = 0;
             for (int c = 0; c < g.Thp; ++c) {
@@ -421,10 +459,8 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             put32(out, (g.pf_phase_idx[t] & 7u) | (nu << 8) | (flags << 16));
             put32(out, (uint32_t)g.pf_power2[t]);
             for (int i = 0; i < 4; ++i) put32(out, (uint32_t)ff[i]);
-            // NodePhases run lengths per rotation class, in run order (j = 0, 2, 1, 3)
-            put32(out, (uint32_t)n_cls[0] | ((uint32_t)n_cls[2] << 16));
-            put32(out, (uint32_t)n_cls[1] | ((uint32_t)n_cls[3] << 16));
-            put64(out, 0);
+            // NodePhases schedule per rotation class, in run order (j = 0, 2, 1, 3)
+            for (int ci = 0; ci < 4; ++ci) put32(out, unsafe ? 0u : np_sched[ci]);
             if (g.pf_has_approx) {
                 double ar = g.pf_approx_f32[2 * (size_t)t], ai = g.pf_approx_f32[2 * (size_t)t + 1];
                 uint64_t u;

@@ -222,7 +222,7 @@ struct TermHdr {
     uint32_t pf_idx, nu_np, flags;
     int32_t power2;
     Zu ff;
-    uint32_t n_cls[4];  // NodePhases run lengths in run order: j = 0, 2, 1, 3
+    uint32_t np_sched[4];  // NodePhases schedule per class in run order j = 0, 2, 1, 3
 };
 
 // The parameter vector's top bit (bit 63 of word W-1) is the constant 1; a
@@ -245,9 +245,7 @@ KS_HD TermHdr load_hdr(const uint8_t *p)
     const int32_t *ff = (const int32_t *)(p + 16);
     h.ff.a = (uint64_t)(int64_t)ff[0]; h.ff.b = (uint64_t)(int64_t)ff[1];
     h.ff.c = (uint64_t)(int64_t)ff[2]; h.ff.d = (uint64_t)(int64_t)ff[3];
-    const uint32_t c0 = u[8], c1 = u[9];
-    h.n_cls[0] = c0 & 0xFFFFu; h.n_cls[1] = c0 >> 16;
-    h.n_cls[2] = c1 & 0xFFFFu; h.n_cls[3] = c1 >> 16;
+    h.np_sched[0] = u[8]; h.np_sched[1] = u[9]; h.np_sched[2] = u[10]; h.np_sched[3] = u[11];
     return h;
 }
 
@@ -301,49 +299,75 @@ KS_HD void ph_update(Zr<T> &z, uint32_t pa, uint32_t pb, uint32_t K)
     }
 }
 
-// A run of NodePhases columns of rotation class J, for S shots: factor
+// One NodePhases column of rotation class J for S shots: factor
 // 1 + (-1)^parity w^J (the mask carries the phase's bit 2 in the constant
-// bit), i.e. z += +-R_J(z); J = 0 is the factor 2 (halved straight back,
-// pw + 1) or 0 (the term dies).  Halvings where the host marked them.
+// bit), i.e. z += +-R_J(z); J = 0 is the factor 2 (pw + 1, halved straight
+// back) or 0 (the term dies, pw frozen at the reference's value).
 template <int W, typename T, int S, int J>
-KS_HD const uint64_t *np_class(const uint64_t *q, uint32_t n, const uint64_t (&v)[S][W], Zr<T> (&z)[S],
-                               int64_t (&pw)[S], uint32_t (&alive)[S])
+KS_HD const uint64_t *np_column(const uint64_t *q, const uint64_t (&v)[S][W], Zr<T> (&z)[S], int64_t (&pw)[S],
+                                uint32_t (&alive)[S])
 {
     constexpr int R1 = rec1_words(W);
-    for (uint32_t t = 0; t < n; ++t, q += R1) {
-        uint64_t r[R1];
-        load_rec<R1>(q, r);
-        uint64_t mw[W];
+    uint64_t r[R1];
+    load_rec<R1>(q, r);
+    uint64_t mw[W];
 #pragma unroll
-        for (int w = 0; w < W; ++w) mw[w] = r[w];
-        uint32_t neg[S];
+    for (int w = 0; w < W; ++w) mw[w] = r[w];
+    uint32_t neg[S];
 #pragma unroll
-        for (int s = 0; s < S; ++s) neg[s] = parity<W>(mw, v[s]);
-        if (J == 0) {
-            // a zero factor freezes pw at the reference's value at this column
-            const int64_t h_before = (int64_t)(((uint32_t)r[W] >> 16) & 0xFFFFu);
+    for (int s = 0; s < S; ++s) neg[s] = parity<W>(mw, v[s]);
+    if (J == 0) {
+        const int64_t h_before = (int64_t)(((uint32_t)r[W] >> 16) & 0xFFFFu);
 #pragma unroll
-            for (int s = 0; s < S; ++s) {
-                pw[s] += (alive[s] & (neg[s] ^ 1u)) + (int64_t)(alive[s] & neg[s]) * h_before;
-                alive[s] &= neg[s] ^ 1u;
-                const T keep = (T)0 - (T)alive[s];
-                z[s].a &= keep; z[s].b &= keep; z[s].c &= keep; z[s].d &= keep;
-            }
-        } else {
+        for (int s = 0; s < S; ++s) {
+            pw[s] += (alive[s] & (neg[s] ^ 1u)) + (int64_t)(alive[s] & neg[s]) * h_before;
+            alive[s] &= neg[s] ^ 1u;
+            const T keep = (T)0 - (T)alive[s];
+            z[s].a &= keep; z[s].b &= keep; z[s].c &= keep; z[s].d &= keep;
+        }
+    } else {
 #pragma unroll
-            for (int s = 0; s < S; ++s) {
-                const Zr<T> t0 = z[s];
-                add_rot(z[s], t0, (uint32_t)J, (T)0 - (T)neg[s]);
-            }
-            if ((uint32_t)r[W] & NP_REDUCE_BIT) {
-#pragma unroll
-                for (int s = 0; s < S; ++s) {
-                    shr_all(z[s], 1u);
-                    pw[s] += alive[s];
-                }
-            }
+        for (int s = 0; s < S; ++s) {
+            const Zr<T> t0 = z[s];
+            add_rot(z[s], t0, (uint32_t)J, (T)0 - (T)neg[s]);
         }
     }
+    return q + R1;
+}
+
+template <typename T, int S>
+KS_HD void halve(Zr<T> (&z)[S], int64_t (&pw)[S], const uint32_t (&alive)[S])
+{
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        shr_all(z[s], 1u);
+        pw[s] += alive[s];
+    }
+}
+
+// The NodePhases columns of class J (schedule word: see image.cpp): head
+// columns and a halving, k unrolled groups of 4 / nu columns each followed by
+// a halving, then tail columns.
+template <int W, typename T, int S, int J>
+KS_HD const uint64_t *np_class(const uint64_t *q, uint32_t sched, const uint64_t (&v)[S][W], Zr<T> (&z)[S],
+                               int64_t (&pw)[S], uint32_t (&alive)[S])
+{
+    if (J == 0) {
+        for (uint32_t t = 0; t < sched; ++t) q = np_column<W, T, S, 0>(q, v, z, pw, alive);
+        return q;
+    }
+    constexpr int GRP = (J & 1) ? 4 : 2;
+    const uint32_t k = sched & 0xFFFFu, head = (sched >> 16) & 15u, tail = (sched >> 20) & 15u;
+    if (head) {
+        for (uint32_t t = 0; t < head; ++t) q = np_column<W, T, S, J>(q, v, z, pw, alive);
+        halve<T, S>(z, pw, alive);
+    }
+    for (uint32_t g = 0; g < k; ++g) {
+#pragma unroll
+        for (int i = 0; i < GRP; ++i) q = np_column<W, T, S, J>(q, v, z, pw, alive);
+        halve<T, S>(z, pw, alive);
+    }
+    for (uint32_t t = 0; t < tail; ++t) q = np_column<W, T, S, J>(q, v, z, pw, alive);
     return q;
 }
 
@@ -371,13 +395,16 @@ KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const ui
 
     // NodePhases: one branch-free loop per rotation class, in the run order
     // the host packed (j = 0, 2, 1, 3)
-    q = np_class<W, T, S, 0>(q, h.n_cls[0], v, z, pw, alive);
-    q = np_class<W, T, S, 2>(q, h.n_cls[1], v, z, pw, alive);
-    q = np_class<W, T, S, 1>(q, h.n_cls[2], v, z, pw, alive);
-    q = np_class<W, T, S, 3>(q, h.n_cls[3], v, z, pw, alive);
-    // HalfPi: w^(sum par*coeff); its renormalisation cannot fire (nu < 4 here)
+    q = np_class<W, T, S, 0>(q, h.np_sched[0], v, z, pw, alive);
+    q = np_class<W, T, S, 2>(q, h.np_sched[1], v, z, pw, alive);
+    q = np_class<W, T, S, 1>(q, h.np_sched[2], v, z, pw, alive);
+    q = np_class<W, T, S, 3>(q, h.np_sched[3], v, z, pw, alive);
+    // HalfPi (w^(sum par*coeff)) and PiProducts (a sign, w^4) are units: they
+    // change no valuation and commute with the PhasePairs factors, so their
+    // rotations are merged with the prefactor's w^idx into one rotation at
+    // the end (the reference's renormalisation after HalfPi cannot fire).
+    uint32_t tot[S];
     {
-        uint32_t tot[S];
 #pragma unroll
         for (int s = 0; s < S; ++s) tot[s] = 0;
         for (uint32_t t = 0; t < h.n_hp; ++t, q += R1) {
@@ -390,10 +417,8 @@ KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const ui
 #pragma unroll
             for (int s = 0; s < S; ++s) tot[s] += parity<W>(mw, v[s]) ? coeff : 0u;
         }
-#pragma unroll
-        for (int s = 0; s < S; ++s) z[s] = rot_var(z[s], tot[s] & 7u);
     }
-    // PiProducts: overall sign
+    // PiProducts: overall sign, kept in tot as w^4
     {
         uint32_t e[S];
 #pragma unroll
@@ -408,10 +433,7 @@ KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const ui
             for (int s = 0; s < S; ++s) e[s] ^= parity<W>(ma, v[s]) & parity<W>(mb, v[s]);
         }
 #pragma unroll
-        for (int s = 0; s < S; ++s) {
-            const T m = (T)0 - (T)e[s];
-            z[s].a = sneg(z[s].a, m); z[s].b = sneg(z[s].b, m); z[s].c = sneg(z[s].c, m); z[s].d = sneg(z[s].d, m);
-        }
+        for (int s = 0; s < S; ++s) tot[s] += 4u * e[s];
     }
     // PhasePairs: per-shot valuation tracking
     {
@@ -457,11 +479,12 @@ KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const ui
             }
         }
     }
-    // prefactor: w^idx, then the exact floatfactor with one renormalisation
+    // prefactor: w^(HalfPi + PiProducts + idx), then the exact floatfactor
+    // with one renormalisation
     const Zr<T> ff = {(T)h.ff.a, (T)h.ff.b, (T)h.ff.c, (T)h.ff.d};
 #pragma unroll
     for (int s = 0; s < S; ++s) {
-        Zr<T> zz = rot_var(z[s], h.pf_idx);
+        Zr<T> zz = rot_var(z[s], (tot[s] + h.pf_idx) & 7u);
         zz = zmul(zz, ff);
         zreduce(zz, pw[s]);
         if constexpr (sizeof(T) == 8) {
