@@ -156,16 +156,31 @@ KS_HD Zr<T> rot_var(Zr<T> z, uint32_t k)
     return q;
 }
 
-// acc += s * R_j(t), s = +1 (m = 0) or -1 (m = ~0), j in 0..3 the same for all shots.
+// The sign (-1)^p in the form the signed adds use, for both orientations:
+// 32-bit words multiply by +-1 (one multiply-add each), 64-bit words
+// xor / subtract with a 0 / ~0 mask.
 template <typename T>
-KS_HD void add_rot(Zr<T> &acc, const Zr<T> &t, uint32_t j, T m)
+struct Sign { T pos, neg; };
+KS_HD Sign<uint32_t> sign_of(uint32_t p, uint32_t) { return {1u - 2u * p, 2u * p - 1u}; }
+KS_HD Sign<uint64_t> sign_of(uint32_t p, uint64_t)
 {
-    const T n = ~m;  // the opposite sign
+    const uint64_t m = 0 - (uint64_t)p;
+    return {m, ~m};
+}
+KS_HD uint32_t sadd(uint32_t acc, uint32_t x, uint32_t s) { return acc + s * x; }
+KS_HD uint64_t sadd(uint64_t acc, uint64_t x, uint64_t m) { return acc + sneg(x, m); }
+
+// acc += (-1)^p * R_j(t), j in 0..3 the same for all shots.
+template <typename T>
+KS_HD void add_rot(Zr<T> &acc, const Zr<T> &t, uint32_t j, uint32_t p)
+{
+    const Sign<T> g = sign_of(p, T());
+    const T m = g.pos, n = g.neg;
     switch (j & 3u) {
-    case 0: acc.a = cadd(acc.a, t.a, m); acc.b = cadd(acc.b, t.b, m); acc.c = cadd(acc.c, t.c, m); acc.d = cadd(acc.d, t.d, m); break;
-    case 1: acc.a = cadd(acc.a, t.d, m); acc.b = cadd(acc.b, t.a, m); acc.c = cadd(acc.c, t.b, m); acc.d = cadd(acc.d, t.c, n); break;
-    case 2: acc.a = cadd(acc.a, t.c, n); acc.b = cadd(acc.b, t.d, m); acc.c = cadd(acc.c, t.a, m); acc.d = cadd(acc.d, t.b, n); break;
-    default: acc.a = cadd(acc.a, t.b, n); acc.b = cadd(acc.b, t.c, n); acc.c = cadd(acc.c, t.d, m); acc.d = cadd(acc.d, t.a, n); break;
+    case 0: acc.a = sadd(acc.a, t.a, m); acc.b = sadd(acc.b, t.b, m); acc.c = sadd(acc.c, t.c, m); acc.d = sadd(acc.d, t.d, m); break;
+    case 1: acc.a = sadd(acc.a, t.d, m); acc.b = sadd(acc.b, t.a, m); acc.c = sadd(acc.c, t.b, m); acc.d = sadd(acc.d, t.c, n); break;
+    case 2: acc.a = sadd(acc.a, t.c, n); acc.b = sadd(acc.b, t.d, m); acc.c = sadd(acc.c, t.a, m); acc.d = sadd(acc.d, t.b, n); break;
+    default: acc.a = sadd(acc.a, t.b, n); acc.b = sadd(acc.b, t.c, n); acc.c = sadd(acc.c, t.d, m); acc.d = sadd(acc.d, t.a, n); break;
     }
 }
 
@@ -286,16 +301,16 @@ template <typename T, int JA, int JB>
 KS_HD void ph_update(Zr<T> &z, uint32_t pa, uint32_t pb, uint32_t K)
 {
     constexpr uint32_t JG = (uint32_t)((JA + JB) & 3);
-    const T ma = (T)0 - (T)pa, mb = (T)0 - (T)pb, mg = (T)0 - (T)(K ^ pa ^ pb);
+    const uint32_t pg = K ^ pa ^ pb;
     const Zr<T> t0 = z;
     if constexpr (JA == 0 && JB == 0) {
-        // a scalar factor 1 + sa + sb + sg
-        const T f = (T)1 + ((T)1 ^ (ma & (T)~(T)1)) + ((T)1 ^ (mb & (T)~(T)1)) + ((T)1 ^ (mg & (T)~(T)1));
+        // a scalar factor 1 + sa + sb + sg = 4 - 2 (pa + pb + pg)
+        const T f = (T)4 - (T)2 * (T)(pa + pb + pg);
         z.a = t0.a * f; z.b = t0.b * f; z.c = t0.c * f; z.d = t0.d * f;
     } else {
-        add_rot(z, t0, (uint32_t)JA, ma);
-        add_rot(z, t0, (uint32_t)JB, mb);
-        add_rot(z, t0, JG, mg);
+        add_rot(z, t0, (uint32_t)JA, pa);
+        add_rot(z, t0, (uint32_t)JB, pb);
+        add_rot(z, t0, JG, pg);
     }
 }
 
@@ -329,7 +344,7 @@ KS_HD const uint64_t *np_column(const uint64_t *q, const uint64_t (&v)[S][W], Zr
 #pragma unroll
         for (int s = 0; s < S; ++s) {
             const Zr<T> t0 = z[s];
-            add_rot(z[s], t0, (uint32_t)J, (T)0 - (T)neg[s]);
+            add_rot(z[s], t0, (uint32_t)J, neg[s]);
         }
     }
     return q + R1;
@@ -435,11 +450,12 @@ KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const ui
 #pragma unroll
         for (int s = 0; s < S; ++s) tot[s] += 4u * e[s];
     }
-    // PhasePairs: per-shot valuation tracking
+    // PhasePairs: after each factor the reference's renormalisation step,
+    // halve once if all four coefficients are even and not all zero
+    // (zx_eval.hpp:35-41).  z here differs from the reference's by a unit
+    // (the NodePhases run order, the deferred HalfPi / PiProducts rotation),
+    // and units preserve evenness, so every decision is the reference's.
     {
-        uint32_t nu[S];
-#pragma unroll
-        for (int s = 0; s < S; ++s) nu[s] = h.nu_np;
         for (uint32_t t = 0; t < h.n_ph; ++t, q += R2) {
             uint64_t r[R2];
             load_rec<R2>(q, r);
@@ -469,11 +485,8 @@ KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const ui
             }
 #pragma unroll
             for (int s = 0; s < S; ++s) {
-                const uint32_t nf = (cw >> (8 + 4 * (pa[s] | (pb[s] << 1)))) & 15u;
-                alive[s] &= (nf != NU_ZERO) ? 1u : 0u;
-                nu[s] += nf;
-                const uint32_t red = alive[s] & (nu[s] >= 4 ? 1u : 0u);
-                nu[s] -= 4 * red;
+                const T o = z[s].a | z[s].b | z[s].c | z[s].d;
+                const uint32_t red = (o != 0 && (o & 1u) == 0) ? 1u : 0u;
                 shr_all(z[s], red);
                 pw[s] += red;
             }
