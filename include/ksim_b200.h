@@ -375,7 +375,8 @@ void ksim_server_destroy(ksim_server *s);
  * the formulation the kernels run (32-bit words for terms proven below 2^31,
  * 64-bit words otherwise, the reference's step-by-step arithmetic for terms
  * on the exact path), and how many terms take each path (paths[0] 32-bit,
- * paths[1] 64-bit, paths[2] exact; nullable).  Host only: no device is
+ * paths[1] 64-bit, paths[2] exact, paths[3] hybrid: NodePhases on 32-bit
+ * words, the rest on 64-bit; nullable, 4 entries).  Host only: no device is
  * needed.  No reference counterpart. */
 ksim_status ksim_work_model(const ksim_graph_desc *graphs, int32_t n_graphs, int32_t num_f,
                             double *ops_per_shot, int64_t *paths);

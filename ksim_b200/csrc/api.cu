@@ -135,8 +135,9 @@ ksim_status ksim_work_model(const ksim_graph_desc *graphs, int32_t n_graphs, int
     *ops_per_shot = img.work_ops;
     if (paths) {
         paths[0] = img.n_narrow_terms;
-        paths[1] = img.n_terms - img.n_narrow_terms - img.n_slow_terms;
+        paths[1] = img.n_terms - img.n_narrow_terms - img.n_slow_terms - img.n_hybrid_terms;
         paths[2] = img.n_slow_terms;
+        paths[3] = img.n_hybrid_terms;
     }
     return KSIM_OK;
 }

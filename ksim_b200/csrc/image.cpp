@@ -106,6 +106,7 @@ bool all_zero(const uint64_t *m, int W)
 // multiplies x 3 + 12 64-bit adds x 2 + renormalisation 12 = 84 per factor).
 //   parity of one W-word mask: 3W (and / xor / fold) + 2 (popcount, bit)
 //   NodePhases j != 0: parity + 1 (sign) + 4c (signed adds) [+ 4c + 1 halving]
+//                      (c = 1 also on the hybrid path, TF_HYBRID)
 //   NodePhases j == 0: parity + 2
 //   HalfPi: parity + 1;  PiProducts: 2 parities + 1
 //   PhasePairs: 2 parities + 3 (signs) + 12c (three rotated adds)
@@ -120,8 +121,9 @@ double term_work(int W, uint32_t flags, const int n_cls[4], int n_hp, int n_pp, 
     if (flags & TF_SLOW)
         return 84.0 * (n_np + n_ph + 3) + par * (n_np + n_hp + 2.0 * n_pp + 2.0 * n_ph) + 16.0;
     const double c = (flags & TF_NARROW) ? 1.0 : 2.0;
+    const double cn = (flags & (TF_NARROW | TF_HYBRID)) ? 1.0 : 2.0;  // NodePhases words
     double w = n_cls[0] * (par + 2.0);
-    w += (n_np - n_cls[0]) * (par + 1.0 + 4.0 * c) + n_halvings * (4.0 * c + 1.0);
+    w += (n_np - n_cls[0]) * (par + 1.0 + 4.0 * cn) + n_halvings * (4.0 * cn + 1.0);
     w += n_hp * (par + 1.0) + n_pp * (2.0 * par + 1.0);
     w += n_ph * (2.0 * par + 3.0 + 12.0 * c + 4.0 + 4.0 * c + 1.0);
     w += 28.0 * c + (c == 1.0 ? 28.0 : 72.0) + 6.0 * c + 16.0;
@@ -360,6 +362,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                     r0 += n;
                 }
             }
+            const double Lmax_np = Lmax;  // the NodePhases block's bound
             // HalfPi
             int n_hp = 0;
             for (int c = 0; c < g.Thp; ++c) {
@@ -442,7 +445,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             }
             // every value the fast path must know exactly is below 2^Lmax; with
             // Lmax <= 30.5 it fits int32 and the term runs on 32-bit words
-            uint32_t flags = unsafe ? TF_SLOW : (Lmax <= 30.5 ? TF_NARROW : 0u);
+            uint32_t flags = unsafe ? TF_SLOW : (Lmax <= 30.5 ? TF_NARROW : (Lmax_np <= 30.5 ? TF_HYBRID : 0u));
             // NodePhases records: class order with halving flags for the fast
             // paths, the reference's order for the exact path
             std::vector<uint8_t> np_rec;
@@ -477,6 +480,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             img.n_terms += 1;
             img.n_slow_terms += unsafe ? 1 : 0;
             img.n_narrow_terms += (flags & TF_NARROW) ? 1 : 0;
+            img.n_hybrid_terms += (flags & TF_HYBRID) ? 1 : 0;
             img.n_columns += n_np + n_hp + n_pp + n_ph;
             img.work_ops += term_work(W, flags, n_cls, n_hp, n_pp, n_ph,
                                       (int)std::count(np_red.begin(), np_red.end(), 1u));

@@ -34,7 +34,7 @@ struct HostImage {
     std::vector<GraphDir> gdir;
     std::vector<std::vector<int64_t>> term_off;  // per graph: term start offsets + end
     int64_t max_term_bytes = 0;
-    int64_t n_terms = 0, n_slow_terms = 0, n_narrow_terms = 0;
+    int64_t n_terms = 0, n_slow_terms = 0, n_narrow_terms = 0, n_hybrid_terms = 0;
     double work_ops = 0;  // int32 operations per shot, all graphs (term_work / graph_work)
     int64_t n_columns = 0;
 };

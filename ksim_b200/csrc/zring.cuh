@@ -43,7 +43,9 @@ namespace ksim {
 // TF_SLOW: evaluate step by step (no proof the fast path stays in range);
 // TF_NARROW: every value the fast path must know exactly (at each halving
 // and at the end) is proven below 2^31, so it runs on 32-bit coefficients.
-enum : uint32_t { TF_SLOW = 1u, TF_APX = 2u, TF_NARROW = 4u };
+// TF_HYBRID: the NodePhases block is proven below 2^31 and runs on 32-bit
+// words, the rest on 64-bit words.
+enum : uint32_t { TF_SLOW = 1u, TF_APX = 2u, TF_NARROW = 4u, TF_HYBRID = 8u };
 constexpr int TERM_HDR_BYTES = 48;
 constexpr int TERM_APX_BYTES = 16;
 // NodePhases / HalfPi column: W mask words + 1 constant word, padded to 16 B
@@ -392,28 +394,39 @@ KS_HD const uint64_t *np_class(const uint64_t *q, uint32_t sched, const uint64_t
 // may leave the narrow range, but the values at each halving and at the end
 // are the true ones.  S shots at once: each column record is loaded and
 // decoded once and applied to S independent parameter vectors.
-template <int W, typename T, int S>
+// TN: word of the NodePhases block, T: word of the rest (TN = uint32_t, T =
+// uint64_t is the hybrid path: NodePhases proven below 2^31, the rest not).
+template <int W, typename TN, typename T, int S>
 KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const uint64_t (&v)[S][W],
                                     TermOut (&o)[S])
 {
     constexpr int R1 = rec1_words(W), R2 = rec2_words(W);
     const uint64_t *q = (const uint64_t *)(p + TERM_HDR_BYTES + ((h.flags & TF_APX) ? TERM_APX_BYTES : 0));
-    Zr<T> z[S];
+    Zr<TN> zn[S];
     int64_t pw[S];
     uint32_t alive[S];
 #pragma unroll
     for (int s = 0; s < S; ++s) {
-        z[s].a = 1; z[s].b = 0; z[s].c = 0; z[s].d = 0;
+        zn[s].a = 1; zn[s].b = 0; zn[s].c = 0; zn[s].d = 0;
         pw[s] = 0;
         alive[s] = 1;
     }
 
     // NodePhases: one branch-free loop per rotation class, in the run order
     // the host packed (j = 0, 2, 1, 3)
-    q = np_class<W, T, S, 0>(q, h.np_sched[0], v, z, pw, alive);
-    q = np_class<W, T, S, 2>(q, h.np_sched[1], v, z, pw, alive);
-    q = np_class<W, T, S, 1>(q, h.np_sched[2], v, z, pw, alive);
-    q = np_class<W, T, S, 3>(q, h.np_sched[3], v, z, pw, alive);
+    q = np_class<W, TN, S, 0>(q, h.np_sched[0], v, zn, pw, alive);
+    q = np_class<W, TN, S, 2>(q, h.np_sched[1], v, zn, pw, alive);
+    q = np_class<W, TN, S, 1>(q, h.np_sched[2], v, zn, pw, alive);
+    q = np_class<W, TN, S, 3>(q, h.np_sched[3], v, zn, pw, alive);
+    Zr<T> z[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        if constexpr (sizeof(TN) == sizeof(T)) {
+            z[s].a = (T)zn[s].a; z[s].b = (T)zn[s].b; z[s].c = (T)zn[s].c; z[s].d = (T)zn[s].d;
+        } else {
+            z[s] = widen(zn[s]);  // sign-extend to the 64-bit words of the rest
+        }
+    }
     // HalfPi (w^(sum par*coeff)) and PiProducts (a sign, w^4) are units: they
     // change no valuation and commute with the PhasePairs factors, so their
     // rotations are merged with the prefactor's w^idx into one rotation at
@@ -605,8 +618,9 @@ KS_HD const uint8_t *eval_term_s(const uint8_t *p, const TermHdr &h, const uint6
         for (int s = 0; s < S; ++s) next = eval_term_exact<W>(p, h, v[s], o[s]);
         return next;
     }
-    if (h.flags & TF_NARROW) return eval_term_fast<W, uint32_t, S>(p, h, v, o);
-    return eval_term_fast<W, uint64_t, S>(p, h, v, o);
+    if (h.flags & TF_NARROW) return eval_term_fast<W, uint32_t, uint32_t, S>(p, h, v, o);
+    if (h.flags & TF_HYBRID) return eval_term_fast<W, uint32_t, uint64_t, S>(p, h, v, o);
+    return eval_term_fast<W, uint64_t, uint64_t, S>(p, h, v, o);
 }
 
 // One term for one shot.

@@ -44,12 +44,12 @@ class HostEmu:
         self.n = len(self.graphs)
 
     def stats(self) -> dict:
-        st = np.zeros(6, np.int64)
+        st = np.zeros(7, np.int64)
         rc = self.L.hostemu_stats(self.descs, self.n, self.F, st.ctypes.data)
         if rc:
             raise ValueError(self.L.hostemu_error().decode())
-        return dict(zip(("W", "terms", "slow_terms", "columns", "max_term_bytes", "narrow_terms"),
-                        st.tolist()))
+        return dict(zip(("W", "terms", "slow_terms", "columns", "max_term_bytes", "narrow_terms",
+                         "hybrid_terms"), st.tolist()))
 
     def eval(self, gi, params, pairs: bool = False) -> np.ndarray:
         """Complex amplitudes; pairs=True evaluates two rows at a time (the

@@ -158,7 +158,7 @@ extern "C" {
 
 const char *hostemu_error(void) { return g_err.c_str(); }
 
-// stats: [W, n_terms, n_slow_terms, n_columns, max_term_bytes, n_narrow_terms]
+// stats: [W, n_terms, n_slow_terms, n_columns, max_term_bytes, n_narrow_terms, n_hybrid_terms]
 int hostemu_stats(const ksim_graph_desc *g, int n, int F, int64_t *stats)
 {
     HostImage img;
@@ -170,6 +170,7 @@ int hostemu_stats(const ksim_graph_desc *g, int n, int F, int64_t *stats)
     stats[3] = img.n_columns;
     stats[4] = img.max_term_bytes;
     stats[5] = img.n_narrow_terms;
+    stats[6] = img.n_hybrid_terms;
     return 0;
 }
 

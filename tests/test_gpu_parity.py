@@ -233,3 +233,24 @@ def test_mixture_distribution(cuda_device):
         for c in range(16):
             p = prob(list(fv), [(c >> j) & 1 for j in range(4)])
             assert abs(counts[c] / m - p) < 5 * math.sqrt(max(p * (1 - p), 1e-12) / m) + 1e-9
+
+
+@pytest.mark.parametrize("Tnp,Tph", [(40, 30), (60, 10)])
+def test_hybrid_and_wide_terms_on_gpu(cuda_device, oracle_port, Tnp, Tph):
+    """Terms whose NodePhases block fits 32-bit words but whose PhasePairs do
+    not (hybrid path), next to 32-bit and 64-bit terms: numerators, amplitudes
+    and bits equal the oracle's."""
+    rng = np.random.default_rng(7000 + Tnp)
+    gs = [synth.random_graph(rng, 6, 20 + k, Tnp, 3, 3, Tph) for k in range(4)]
+    comp = FlatComponent((0, 1, 2), np.arange(20, dtype=np.int32), gs)
+    kc = _component(comp.graphs, 20)
+    po = oracle_port.PortOracle(comp.graphs, 20)
+    for gi, g in enumerate(comp.graphs):
+        pv = rng.integers(0, 2, size=(129, g.np_params.shape[2])).astype(np.uint8)
+        assert np.array_equal(kc.eval_terms(gi, pv), po.eval_terms(gi, pv)), gi
+        assert same_bits(kc.eval(gi, pv), po.eval(gi, pv)), gi
+    f = synth.sample_f(rng, 2000, 20, 0.1)
+    for mode in (0, 1):
+        want, want_amp = po.sample(f, 99, mode, return_amp=True)
+        bits, amp = device_sample(kc, f, 99, mode)
+        assert np.array_equal(bits, want[:, :kc.n_out]) and same_bits(amp, want_amp)

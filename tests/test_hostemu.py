@@ -41,7 +41,7 @@ def test_random_components(hostemu, oracle_port, seed):
     _check_component(hostemu, oracle_port, comp, int(np.asarray(comp.f_selection).shape[0]), rng)
 
 
-@pytest.mark.parametrize("Tnp,Tph", [(24, 4), (60, 10), (130, 20), (250, 40)])
+@pytest.mark.parametrize("Tnp,Tph", [(24, 4), (40, 30), (60, 10), (130, 20), (250, 40)])
 def test_long_terms_exact_path(hostemu, oracle_port, Tnp, Tph):
     """Short terms run on 32-bit words, longer ones on 64-bit words, and terms
     the host cannot prove overflow-free take the exact path."""
@@ -49,16 +49,16 @@ def test_long_terms_exact_path(hostemu, oracle_port, Tnp, Tph):
     gs = [synth.random_graph(rng, 4, 20 + k, Tnp, 3, 3, Tph) for k in range(4)]
     comp = FlatComponent((0, 1, 2), np.arange(20, dtype=np.int32), gs)
     st = _check_component(hostemu, oracle_port, comp, 20, rng, B=32)
-    wide = st["terms"] - st["slow_terms"] - st["narrow_terms"]
+    wide = st["terms"] - st["slow_terms"] - st["narrow_terms"] - st["hybrid_terms"]
     if Tnp == 24:
         assert st["narrow_terms"] == st["terms"]
     if Tnp == 60:
-        assert wide > 0
+        assert wide + st["hybrid_terms"] > 0
     if Tnp >= 250:
         assert st["slow_terms"] == st["terms"]
 
 
-@pytest.mark.parametrize("Tnp,Tph", [(24, 4), (60, 10), (250, 40)])
+@pytest.mark.parametrize("Tnp,Tph", [(24, 4), (40, 30), (60, 10), (250, 40)])
 def test_two_shots_per_thread_path(hostemu, oracle_port, Tnp, Tph):
     """Evaluating two parameter rows at once (the kernels' two-shots-per-thread
     path, on the 32-bit, 64-bit and exact term paths) gives the same
@@ -78,14 +78,15 @@ def test_two_shots_per_thread_path(hostemu, oracle_port, Tnp, Tph):
 
 def test_every_term_path_is_taken(hostemu):
     """The parametrised components above cover the 32-bit, 64-bit and exact paths."""
-    counts = {"narrow": 0, "wide": 0, "slow": 0}
-    for Tnp, Tph in [(24, 4), (60, 10), (130, 20), (250, 40)]:
+    counts = {"narrow": 0, "hybrid": 0, "wide": 0, "slow": 0}
+    for Tnp, Tph in [(24, 4), (40, 30), (60, 10), (130, 20), (250, 40)]:
         rng = np.random.default_rng(Tnp)
         gs = [synth.random_graph(rng, 4, 20 + k, Tnp, 3, 3, Tph) for k in range(4)]
         st = HostEmu(hostemu, gs, 20).stats()
         counts["narrow"] += st["narrow_terms"]
+        counts["hybrid"] += st["hybrid_terms"]
         counts["slow"] += st["slow_terms"]
-        counts["wide"] += st["terms"] - st["narrow_terms"] - st["slow_terms"]
+        counts["wide"] += st["terms"] - st["narrow_terms"] - st["slow_terms"] - st["hybrid_terms"]
     assert all(v > 0 for v in counts.values()), counts
 
 
