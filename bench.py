@@ -207,6 +207,18 @@ def cpu_reference_rate(prog, f, seed, rng_mode, target_s, max_shots):
     return n2 / dt, kind, threads, n2, dt
 
 
+def arm_config(w, shots, n_f, rng, world):
+    """The config object both arms print (same workload, same keys)."""
+    n_out = int(len(w.program.output_order))
+    terms = sum(int(g.pf_phase_idx.shape[0]) for c in w.program.components for g in c.graphs)
+    graphs = sum(len(c.graphs) for c in w.program.components)
+    return {"workload": f"{w.name}: {n_out} outputs, F={n_f}, {terms} terms/shot over {graphs} graphs",
+            "shots_per_gpu": shots,
+            "rng": "xorshift (kokkos_sim stream)" if rng == 0 else "philox4x32-10",
+            "l2": "flushed between steps (256 MiB write)",
+            "parallelism": f"shot-split x{world}"}
+
+
 def run_reference(args):
     world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
     if rank != 0:
@@ -240,7 +252,8 @@ def run_reference(args):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-            "config": {"workload": w.name, "shots_per_gpu": shots, "step_shots": step_shots},
+            "config": arm_config(w, shots, f.shape[1], args.rng, args.gpus),
+            "step_shots": step_shots,
             "cpu_baseline": {"value": value, "unit": "shots/s", "cores": threads, "kind": kind,
                              "sample": sample},
             "e2e": {"value": value, "unit": "shots/s", "h2d_bytes_per_step": 0,
@@ -555,12 +568,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
             "data": "synthetic",
-            "config": {"workload": f"{w.name}: {n_out} outputs, F={n_f}, "
-                                   f"{work['terms']} terms/shot over {work['graphs']} graphs",
-                       "shots_per_gpu": shots,
-                       "rng": "xorshift (kokkos_sim stream)" if args.rng == 0 else "philox4x32-10",
-                       "l2": "flushed between steps (256 MiB write)",
-                       "parallelism": f"shot-split x{world}"},
+            "config": arm_config(w, shots, n_f, args.rng, world),
             "e2e": {"value": e2e_value, "unit": "shots/s", "h2d_bytes_per_step": int(f.nbytes),
                     "d2h_bytes_per_step": int(shots * n_out),
                     "api": "B200ProgramSampler.sample (ksim_program_sample), pinned buffers"},
