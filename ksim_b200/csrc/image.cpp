@@ -3,15 +3,17 @@
 // Input: the reference's per-graph arrays (sampler.py:21-43 dict layout,
 // kokkos_sim.cpp:91-129 field set).  Output: one byte image
 //   [GraphDir x n_graphs][term stream of graph 0][term stream of graph 1]...
-// Each term record (16-byte aligned):
-//   u32 n_np | n_hp<<16, u32 n_pp | n_ph<<16, u32 pf_idx | nu_np<<8 | flags<<16,
-//   i32 power2, i32 floatfactor[4], [f64 approx re, im], then the columns.
-// Column records hold the parameter masks as W 64-bit words (bit j = param j)
-// and one constant word:
-//   NodePhases  [mask W][phase | reduce<<3]               (count = np_counts[g])
-//   HalfPi      [mask W][coeff & 7]                       (zero coeffs dropped)
-//   PiProducts  [psi W][phi W][psi_c | phi_c<<1]          (identically-zero dropped)
-//   PhasePairs  [alpha W][beta W][a | b<<3 | nu table<<8] (count = ph_counts[g])
+// Each term record (16-byte aligned), a 48-byte header:
+//   u32 n_np | n_hp<<16, u32 n_pp | n_ph<<16, u32 pf_idx | flags<<16,
+//   i32 power2, i32 floatfactor[4], u32 NodePhases schedule[4] (one word per
+//   rotation class, see below), then [f64 approx re, im], then the columns.
+// Column records hold the parameter masks as W 64-bit words (bit j = param j;
+// the top bit of word W-1 is the constant 1 of the parameter vector, set in a
+// mask when the column's constant is 1) and one constant word:
+//   NodePhases  [mask W][phase | reduce<<3 | h_before<<16]   (count = np_counts[g])
+//   HalfPi      [mask W][coeff & 7]                          (zero coeffs dropped)
+//   PiProducts  [psi W][phi W][psi_c | phi_c<<1]             (identically-zero dropped)
+//   PhasePairs  [alpha W][beta W][ja | K<<2 | jb<<3 | jg<<5] (count = ph_counts[g])
 // Dropped columns contribute nothing in the reference either (a zero HalfPi
 // coefficient adds 0 to the phase sum; a PiProducts column whose psi or phi is
 // identically 0 adds psi*phi = 0).
@@ -421,8 +423,6 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 for (uint32_t combo = 0; combo < 4; ++combo) {  // combo = raw pa | pb << 1
                     int64_t f[4];
                     phase_pair((int)(ac ^ ((combo & 1u) << 2)), (int)(bc ^ ((combo >> 1) << 2)), f);
-                    const uint32_t folded = combo ^ (a2 | (b2 << 1));  // index pa' | pb' << 1
-                    cw |= (uint64_t)zw_valuation(f) << (8 + 4 * folded);
                     fmax = std::max(fmax, max_embed(f));
                 }
                 step(L + 2.0);  // partial sums of four rotated copies
@@ -459,7 +459,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             if (g.pf_has_approx) flags |= TF_APX;
             put32(out, (uint32_t)n_np | ((uint32_t)n_hp << 16));
             put32(out, (uint32_t)n_pp | ((uint32_t)n_ph << 16));
-            put32(out, (g.pf_phase_idx[t] & 7u) | (nu << 8) | (flags << 16));
+            put32(out, (g.pf_phase_idx[t] & 7u) | (flags << 16));
             put32(out, (uint32_t)g.pf_power2[t]);
             for (int i = 0; i < 4; ++i) put32(out, (uint32_t)ff[i]);
             // NodePhases schedule per rotation class, in run order (j = 0, 2, 1, 3)

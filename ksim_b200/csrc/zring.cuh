@@ -207,8 +207,8 @@ KS_HD void shr_all(Zr<T> &z, uint32_t n)
 KS_HD void shr1_all(Zu &z) { shr_all(z, 1u); }
 
 // One renormalisation step with the explicit test (zx_eval.hpp:35-41).
-template <typename T>
-KS_HD void zreduce(Zr<T> &z, int64_t &pw)
+template <typename T, typename P>
+KS_HD void zreduce(Zr<T> &z, P &pw)
 {
     const T o = z.a | z.b | z.c | z.d;
     if (o != 0 && (o & 1u) == 0) {
@@ -236,7 +236,7 @@ KS_HD bool over62(const Zu &z)
 
 struct TermHdr {
     uint32_t n_np, n_hp, n_pp, n_ph;
-    uint32_t pf_idx, nu_np, flags;
+    uint32_t pf_idx, flags;
     int32_t power2;
     Zu ff;
     uint32_t np_sched[4];  // NodePhases schedule per class in run order j = 0, 2, 1, 3
@@ -257,7 +257,7 @@ KS_HD TermHdr load_hdr(const uint8_t *p)
     TermHdr h;
     h.n_np = w0 & 0xFFFFu; h.n_hp = w0 >> 16;
     h.n_pp = w1 & 0xFFFFu; h.n_ph = w1 >> 16;
-    h.pf_idx = w2 & 7u; h.nu_np = (w2 >> 8) & 0xFFu; h.flags = (w2 >> 16) & 0xFFu;
+    h.pf_idx = w2 & 7u; h.flags = (w2 >> 16) & 0xFFu;
     h.power2 = (int32_t)u[3];
     const int32_t *ff = (const int32_t *)(p + 16);
     h.ff.a = (uint64_t)(int64_t)ff[0]; h.ff.b = (uint64_t)(int64_t)ff[1];
@@ -321,7 +321,7 @@ KS_HD void ph_update(Zr<T> &z, uint32_t pa, uint32_t pb, uint32_t K)
 // bit), i.e. z += +-R_J(z); J = 0 is the factor 2 (pw + 1, halved straight
 // back) or 0 (the term dies, pw frozen at the reference's value).
 template <int W, typename T, int S, int J>
-KS_HD const uint64_t *np_column(const uint64_t *q, const uint64_t (&v)[S][W], Zr<T> (&z)[S], int64_t (&pw)[S],
+KS_HD const uint64_t *np_column(const uint64_t *q, const uint64_t (&v)[S][W], Zr<T> (&z)[S], int32_t (&pw)[S],
                                 uint32_t (&alive)[S])
 {
     constexpr int R1 = rec1_words(W);
@@ -334,10 +334,10 @@ KS_HD const uint64_t *np_column(const uint64_t *q, const uint64_t (&v)[S][W], Zr
 #pragma unroll
     for (int s = 0; s < S; ++s) neg[s] = parity<W>(mw, v[s]);
     if (J == 0) {
-        const int64_t h_before = (int64_t)(((uint32_t)r[W] >> 16) & 0xFFFFu);
+        const int32_t h_before = (int32_t)(((uint32_t)r[W] >> 16) & 0xFFFFu);
 #pragma unroll
         for (int s = 0; s < S; ++s) {
-            pw[s] += (alive[s] & (neg[s] ^ 1u)) + (int64_t)(alive[s] & neg[s]) * h_before;
+            pw[s] += (int32_t)(alive[s] & (neg[s] ^ 1u)) + (int32_t)(alive[s] & neg[s]) * h_before;
             alive[s] &= neg[s] ^ 1u;
             const T keep = (T)0 - (T)alive[s];
             z[s].a &= keep; z[s].b &= keep; z[s].c &= keep; z[s].d &= keep;
@@ -353,12 +353,12 @@ KS_HD const uint64_t *np_column(const uint64_t *q, const uint64_t (&v)[S][W], Zr
 }
 
 template <typename T, int S>
-KS_HD void halve(Zr<T> (&z)[S], int64_t (&pw)[S], const uint32_t (&alive)[S])
+KS_HD void halve(Zr<T> (&z)[S], int32_t (&pw)[S], const uint32_t (&alive)[S])
 {
 #pragma unroll
     for (int s = 0; s < S; ++s) {
         shr_all(z[s], 1u);
-        pw[s] += alive[s];
+        pw[s] += (int32_t)alive[s];
     }
 }
 
@@ -367,7 +367,7 @@ KS_HD void halve(Zr<T> (&z)[S], int64_t (&pw)[S], const uint32_t (&alive)[S])
 // a halving, then tail columns.
 template <int W, typename T, int S, int J>
 KS_HD const uint64_t *np_class(const uint64_t *q, uint32_t sched, const uint64_t (&v)[S][W], Zr<T> (&z)[S],
-                               int64_t (&pw)[S], uint32_t (&alive)[S])
+                               int32_t (&pw)[S], uint32_t (&alive)[S])
 {
     if (J == 0) {
         for (uint32_t t = 0; t < sched; ++t) q = np_column<W, T, S, 0>(q, v, z, pw, alive);
@@ -403,7 +403,7 @@ KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const ui
     constexpr int R1 = rec1_words(W), R2 = rec2_words(W);
     const uint64_t *q = (const uint64_t *)(p + TERM_HDR_BYTES + ((h.flags & TF_APX) ? TERM_APX_BYTES : 0));
     Zr<TN> zn[S];
-    int64_t pw[S];
+    int32_t pw[S];  // halvings within one term stay far below 2^31
     uint32_t alive[S];
 #pragma unroll
     for (int s = 0; s < S; ++s) {
@@ -501,7 +501,7 @@ KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const ui
                 const T o = z[s].a | z[s].b | z[s].c | z[s].d;
                 const uint32_t red = (o != 0 && (o & 1u) == 0) ? 1u : 0u;
                 shr_all(z[s], red);
-                pw[s] += red;
+                pw[s] += (int32_t)red;
             }
         }
     }
@@ -518,7 +518,7 @@ KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const ui
         } else {
             o[s].z = widen(zz);
         }
-        o[s].pw = pw[s];
+        o[s].pw = (int64_t)pw[s];
         o[s].power2 = h.power2;
         o[s].risk = 0;
     }
