@@ -72,3 +72,13 @@ def test_packed_io_equals_byte_io(cuda_device, small_prog, B):
         assert np.array_equal(unpacked, want)
     with pytest.raises(ValueError):
         s.sample_packed(np.zeros((3, 1), np.uint8), n_f + 9, 1)
+
+
+def test_packed_io_without_f_columns(cuda_device):
+    from ksim_b200.sampler import B200ProgramSampler
+    rng = np.random.default_rng(12)
+    prog = synth.single_component_program(synth.random_component(rng, n_out=11, F=0, t=3))
+    s = B200ProgramSampler(prog, device=0)
+    want = s.sample(np.zeros((3001, 0), np.uint8), 9)
+    got = s.sample_packed(np.zeros((3001, 0), np.uint8), 0, 9)
+    assert np.array_equal(got, np.packbits(want, axis=1, bitorder="little"))

@@ -54,3 +54,23 @@ def test_sample_noisy_equals_sampling_the_drawn_f(cuda_device, oracle_port):
             assert np.array_equal(s.sample_noisy(ns, B, 77, rng_mode=mode), s.sample(f, 77, rng_mode=mode))
     with pytest.raises(ValueError):
         s.sample_noisy(DeviceChannelSampler(probs, T[:3], seed=1), 10, 1)
+
+
+def test_noise_edge_cases(cuda_device, oracle_port):
+    """No channels, channels that never fire, no f parameters, and a program
+    without f parameters sampled through an empty model."""
+    from ksim_b200.noise import DeviceChannelSampler
+    from ksim_b200.sampler import B200ProgramSampler
+    empty = DeviceChannelSampler([], np.zeros((5, 0), np.uint8), seed=3)
+    assert empty.num_channels == 0 and not empty.sample(100).any()
+    never = DeviceChannelSampler([np.array([1.0, 0.0]), np.array([1.0, 0, 0, 0])],
+                                 np.ones((4, 3), np.uint8), seed=3)
+    assert never.num_channels == 0 and not never.sample(100).any()
+    nof = DeviceChannelSampler([np.array([0.5, 0.5])], np.zeros((0, 1), np.uint8), seed=3)
+    assert nof.sample(10).shape == (10, 0)
+    rng = np.random.default_rng(8)
+    comp = synth.random_component(rng, n_out=4, F=0, t=4)
+    prog = synth.single_component_program(comp)
+    s = B200ProgramSampler(prog, device=0)
+    assert np.array_equal(s.sample_noisy(nof, 777, 5), s.sample(np.zeros((777, 0), np.uint8), 5))
+    assert s.sample_noisy(nof, 0, 5).shape == (0, prog.num_outputs)
