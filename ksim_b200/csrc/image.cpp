@@ -3,14 +3,16 @@
 // Input: the reference's per-graph arrays (sampler.py:21-43 dict layout,
 // kokkos_sim.cpp:91-129 field set).  Output: one byte image
 //   [GraphDir x n_graphs][term stream of graph 0][term stream of graph 1]...
-// Each term record (16-byte aligned), a 48-byte header:
+// Each term record (16-byte aligned), an 80-byte header:
 //   u32 n_np | n_hp<<16, u32 n_pp | n_ph<<16, u32 pf_idx | flags<<16,
-//   i32 power2, i32 floatfactor[4], u32 NodePhases schedule[4] (one word per
-//   rotation class, see below), then [f64 approx re, im], then the columns.
+//   i32 power2, i32 floatfactor[4], u32 n0 | n2<<16, u32 n1 | n3<<16 (the
+//   NodePhases columns per rotation class), i32 H (the block's halvings),
+//   u32 0, u64 C[4] (the block's all-plus product / 2^H, mod 2^64),
+//   then [f64 approx re, im], then the columns.
 // Column records hold the parameter masks as W 64-bit words (bit j = param j;
 // the top bit of word W-1 is the constant 1 of the parameter vector, set in a
 // mask when the column's constant is 1) and one constant word:
-//   NodePhases  [mask W][phase | reduce<<3 | h_before<<16]   (count = np_counts[g])
+//   NodePhases  [mask W][phase | dead_pw<<16]                (count = np_counts[g])
 //   HalfPi      [mask W][coeff & 7]                          (zero coeffs dropped)
 //   PiProducts  [psi W][phi W][psi_c | phi_c<<1]             (identically-zero dropped)
 //   PhasePairs  [alpha W][beta W][ja | K<<2 | jb<<3 | jg<<5] (count = ph_counts[g])
@@ -116,7 +118,7 @@ bool all_zero(const uint64_t *m, int W)
 //   per term: rotations and signs 28c, floatfactor product 28 (c = 1) or
 //             72 (c = 2), renormalisation 6c, complex value and sum 16
 //   per graph: parameter vector 4W + 8, Bernoulli step 10
-double term_work(int W, uint32_t flags, const int n_cls[4], int n_hp, int n_pp, int n_ph, int n_halvings)
+double term_work(int W, uint32_t flags, const int n_cls[4], int n_hp, int n_pp, int n_ph)
 {
     const double par = 3.0 * W + 2.0;
     const int n_np = n_cls[0] + n_cls[1] + n_cls[2] + n_cls[3];
@@ -124,8 +126,11 @@ double term_work(int W, uint32_t flags, const int n_cls[4], int n_hp, int n_pp, 
         return 84.0 * (n_np + n_ph + 3) + par * (n_np + n_hp + 2.0 * n_pp + 2.0 * n_ph) + 16.0;
     const double c = (flags & TF_NARROW) ? 1.0 : 2.0;
     const double cn = (flags & (TF_NARROW | TF_HYBRID)) ? 1.0 : 2.0;  // NodePhases words
-    double w = n_cls[0] * (par + 2.0);
-    w += (n_np - n_cls[0]) * (par + 1.0 + 4.0 * cn) + n_halvings * (4.0 * cn + 1.0);
+    // NodePhases: a parity and a count (class 0: a parity and a kill test)
+    // per column, then C * lambda^e (a table read and a product) per term
+    double w = n_cls[0] * (par + 2.0) + (n_np - n_cls[0]) * (par + 1.0);
+    if (n_cls[1] | n_cls[3]) w += 16.0 * cn + 2.0;
+    w += 4.0 * cn + 4.0;
     w += n_hp * (par + 1.0) + n_pp * (2.0 * par + 1.0);
     w += n_ph * (2.0 * par + 3.0 + 12.0 * c + 4.0 + 4.0 * c + 1.0);
     w += 28.0 * c + (c == 1.0 ? 28.0 : 72.0) + 6.0 * c + 16.0;
@@ -295,21 +300,26 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             int n_cls[4] = {0, 0, 0, 0};
             for (int c = 0; c < cnp; ++c) ++n_cls[npc[c].phase & 3u];
             // A term whose factor 2 / 0 column yields 0 keeps the pw the
-            // reference had at that column: its surviving earlier factor-2
-            // columns (counted at run time, they run first in their original
-            // relative order) plus the halvings before the column in the
-            // reference's order, stored in the column word.
-            std::vector<uint32_t> h_before((size_t)cnp, 0);
+            // reference had at that column: its earlier factor-2 columns plus
+            // the halvings before it in the reference's order (dead_pw, stored
+            // in the column word; class-0 columns keep their relative order).
+            std::vector<uint32_t> dead_pw((size_t)cnp, 0);
             {
-                uint32_t cum = 0;
+                uint32_t cum = 0, n_two = 0;
                 for (int c = 0; c < cnp; ++c) {
                     const uint32_t j = npc[c].phase & 3u;
-                    h_before[c] = cum / 4;
+                    dead_pw[c] = n_two + cum / 4;
                     if (j) cum += (j & 1u) ? 1u : 2u;
+                    else ++n_two;
                 }
             }
+            // Bound and halving points of the block in run order; C is the
+            // all-plus product with the same halvings (class 0 contributes
+            // 2 / 2 = 1).
             std::vector<uint32_t> np_red((size_t)cnp, 0);  // halving flag, by run position
             uint32_t nu = 0;
+            __int128 C[4] = {1, 0, 0, 0};
+            bool c_ok = true;
             for (int r = 0; r < cnp; ++r) {
                 const uint32_t j = npc[order[r]].phase & 3u;
                 if (j == 0) {
@@ -318,52 +328,26 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                     nu += (j & 1u) ? 1u : 2u;
                     L += (j & 1u) ? std::log2(2.0 * std::cos(M_PI / 8)) : 0.5;
                     step(L);
+                    // C *= 1 + w^j: w = (0,1,0,0), i = (0,0,1,0), w^3 = (0,0,0,-1)
+                    const __int128 a = C[0], b = C[1], c = C[2], d = C[3];
+                    if (j == 1) { C[0] = a + d; C[1] = b + a; C[2] = c + b; C[3] = d - c; }
+                    else if (j == 2) { C[0] = a - c; C[1] = b + d; C[2] = c + a; C[3] = d - b; }
+                    else { C[0] = a - b; C[1] = b - c; C[2] = c + d; C[3] = d - a; }
                     if (nu >= 4) {
                         nu -= 4;
                         np_red[r] = 1;
                         L -= 1.0;
+                        for (int k = 0; k < 4; ++k) {
+                            if (C[k] & 1) c_ok = false;
+                            C[k] >>= 1;
+                        }
                     }
+                    for (int k = 0; k < 4; ++k)
+                        if (C[k] > ((__int128)1 << 100) || C[k] < -((__int128)1 << 100)) c_ok = false;
                 }
             }
             const int n_np = cnp;
-            // Halvings inside a class run are periodic (every 4 columns for
-            // j odd, nu = 1; every 2 for j = 2, nu = 2) once the first has
-            // happened, so each class is encoded as head columns (then a
-            // halving), k groups of 4 / nu columns (each followed by a
-            // halving) and tail columns: word = k | head << 16 | tail << 20.
-            // j = 0 columns never halve: word = their count.
-            uint32_t np_sched[4] = {0, 0, 0, 0};
-            {
-                static const uint32_t kRunClass[4] = {0, 2, 1, 3};
-                int r0 = 0;
-                for (int ci = 0; ci < 4; ++ci) {
-                    const uint32_t j = kRunClass[ci];
-                    const int n = n_cls[j];
-                    if (j == 0) {
-                        np_sched[ci] = (uint32_t)n;
-                        r0 += n;
-                        continue;
-                    }
-                    const int grp = (j & 1u) ? 4 : 2;
-                    std::vector<int> hv;  // halving positions within the class
-                    for (int i = 0; i < n; ++i)
-                        if (np_red[r0 + i]) hv.push_back(i);
-                    int head = 0, k = 0, tail = n;
-                    if (!hv.empty()) {
-                        head = hv[0] + 1;
-                        k = (int)hv.size() - 1;
-                        tail = n - head - k * grp;
-                        for (int h = 1; h < (int)hv.size(); ++h)
-                            if (hv[h] != hv[0] + h * grp) tail = -1;
-                    }
-                    if (head > grp || tail < 0 || tail >= grp + (hv.empty() ? 0 : 0) || k > 0xFFFF) {
-                        err = gname + ": internal error: NodePhases halving schedule is not periodic";
-                        return KSIM_ERR_INTERNAL;
-                    }
-                    np_sched[ci] = (uint32_t)k | ((uint32_t)head << 16) | ((uint32_t)tail << 20);
-                    r0 += n;
-                }
-            }
+            const int32_t np_halvings = n_cls[0] + (int32_t)std::count(np_red.begin(), np_red.end(), 1u);
             const double Lmax_np = Lmax;  // the NodePhases block's bound
             // HalfPi
             int n_hp = 0;
@@ -445,15 +429,20 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             }
             // every value the fast path must know exactly is below 2^Lmax; with
             // Lmax <= 30.5 it fits int32 and the term runs on 32-bit words
+            // (a fast term's odd classes are far below LAM_MAX columns: each
+            // adds about 0.64 to the bound; the check keeps the table lookup
+            // in range whatever the bound)
+            uint32_t max_dead = 0;
+            for (uint32_t d : dead_pw) max_dead = std::max(max_dead, d);
+            if (std::max(n_cls[1], n_cls[3]) > LAM_MAX || !c_ok || max_dead > 0xFFFFu) unsafe = true;
             uint32_t flags = unsafe ? TF_SLOW : (Lmax <= 30.5 ? TF_NARROW : (Lmax_np <= 30.5 ? TF_HYBRID : 0u));
-            // NodePhases records: class order with halving flags for the fast
-            // paths, the reference's order for the exact path
+            // NodePhases records: class order for the fast paths, the
+            // reference's order for the exact path
             std::vector<uint8_t> np_rec;
             for (int r = 0; r < cnp; ++r) {
                 const int c = unsafe ? r : order[r];
                 for (int w = 0; w < W; ++w) put64(np_rec, npc[c].m[w]);
-                put64(np_rec, (uint64_t)npc[c].phase | ((!unsafe && np_red[r]) ? NP_REDUCE_BIT : 0u) |
-                                  ((uint64_t)std::min<uint32_t>(h_before[c], 0xFFFFu) << 16));
+                put64(np_rec, (uint64_t)npc[c].phase | (unsafe ? 0ull : (uint64_t)dead_pw[c] << 16));
                 for (int w = W + 1; w < R1; ++w) put64(np_rec, 0);
             }
             if (g.pf_has_approx) flags |= TF_APX;
@@ -462,8 +451,12 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             put32(out, (g.pf_phase_idx[t] & 7u) | (flags << 16));
             put32(out, (uint32_t)g.pf_power2[t]);
             for (int i = 0; i < 4; ++i) put32(out, (uint32_t)ff[i]);
-            // NodePhases schedule per rotation class, in run order (j = 0, 2, 1, 3)
-            for (int ci = 0; ci < 4; ++ci) put32(out, unsafe ? 0u : np_sched[ci]);
+            // NodePhases class counts in run order (j = 0, 2, 1, 3), H and C
+            put32(out, (uint32_t)n_cls[0] | ((uint32_t)n_cls[2] << 16));
+            put32(out, (uint32_t)n_cls[1] | ((uint32_t)n_cls[3] << 16));
+            put32(out, unsafe ? 0u : (uint32_t)np_halvings);
+            put32(out, 0u);
+            for (int k = 0; k < 4; ++k) put64(out, unsafe ? 0ull : (uint64_t)C[k]);
             if (g.pf_has_approx) {
                 double ar = g.pf_approx_f32[2 * (size_t)t], ai = g.pf_approx_f32[2 * (size_t)t + 1];
                 uint64_t u;
@@ -482,8 +475,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             img.n_narrow_terms += (flags & TF_NARROW) ? 1 : 0;
             img.n_hybrid_terms += (flags & TF_HYBRID) ? 1 : 0;
             img.n_columns += n_np + n_hp + n_pp + n_ph;
-            img.work_ops += term_work(W, flags, n_cls, n_hp, n_pp, n_ph,
-                                      (int)std::count(np_red.begin(), np_red.end(), 1u));
+            img.work_ops += term_work(W, flags, n_cls, n_hp, n_pp, n_ph);
         }
         toff.push_back((int64_t)out.size());
         img.work_ops += graph_work(W);

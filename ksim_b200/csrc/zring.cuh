@@ -9,32 +9,43 @@
 //   w^2: (-c,  d,  a, -b)      w^3: (-b, -c,  d, -a)      w^(j+4) = -w^j
 // so every family factor except the floatfactor is a few adds, not a 16-multiply
 // product:
-//   NodePhases  (1 + w^k), k = phase ^ 4*par  ->  z + s*R_j(z), s = +-1 per shot
 //   PhasePairs  1 + w^a + w^b - w^(a+b)        ->  z + sa*R(z) + sb*R(z) + sc*R(z)
 //   HalfPi / phase index: a rotation; PiProducts: a sign.
+//
+// NodePhases need no per-column arithmetic at all.  A column's factor is
+// 1 + s w^j (s = +-1 from the parity), and 1 - x = (1 + x) u with a unit u:
+//   j = 2: u = w^6,   j = 1: u = w^6 / lambda,   j = 3: u = w^6 lambda,
+// lambda = 1 + sqrt2 = 1 + w + conj w.  With m_j the number of columns of
+// class j whose sign is -1, the block's product is
+//   2^n0 (1 + i)^n2 (1 + w)^n1 (1 + w^3)^n3 * w^(6 (m1 + m2 + m3)) * lambda^(m3 - m1)
+// or 0 if a class-0 column (factor 1 + s = 2 or 0) has s = -1.  Every factor
+// has (1 - w)-adic valuation <= 4 and the reference halves at most once per
+// factor, so it divides the product by 2^H, H = floor(sum nu / 4), whatever
+// the signs.  The host folds the all-plus product / 2^H into one constant C
+// per term; a shot counts its m_j, reads lambda^(m3 - m1) from a table and
+// makes one product, and the rotation joins the deferred one at the end.
 //
 // Renormalisation ("halve when all four are even and not all zero",
 // zx_eval.hpp:35-41) is decided without looking at the coefficients: for
 // nonzero z, all four are even  <=>  nu(z) >= 4, where nu is the
 // (1 - w)-adic valuation (2 = unit * (1 - w)^4), and nu is additive under
-// products.  The NodePhases factors have nu = 1 (j odd), 2 (j = 2), 4 (j = 0,
-// value 2) or are zero, so within the NodePhases block the halving steps are
-// the same for every shot and the host precomputes them (bit 3 of the column
-// word).  PhasePairs factors depend on the shot's parities; their nu for each
-// of the four parity combinations is tabulated by the host in the column word
-// and tracked per shot.  This reproduces the reference's (a, b, c, d, pw)
-// exactly whenever no coefficient leaves the int64 range; the host proves
-// that per term from an embedding-norm bound (|coefficient| <= max_k
-// |sigma_k(z)|), and terms it cannot prove safe are evaluated by
-// eval_term_exact, the reference's step-by-step arithmetic including the
-// explicit evenness test and int64 wrap.
+// products.  PhasePairs factors depend on the shot's parities and take the
+// explicit test per shot.  This reproduces the reference's (a, b, c, d, pw)
+// exactly whenever no coefficient leaves the int64 range (all the fast path's
+// arithmetic wraps like the reference's, and only a halving or the end needs
+// the true value); the host proves that per term from an embedding-norm bound
+// (|coefficient| <= max_k |sigma_k(z)|), and terms it cannot prove safe are
+// evaluated by eval_term_exact, the reference's step-by-step arithmetic
+// including the explicit evenness test and int64 wrap.
 #pragma once
 #include <stdint.h>
 
 #if defined(__CUDACC__)
 #define KS_HD __host__ __device__ __forceinline__
+#define KS_CE __host__ __device__ constexpr
 #else
 #define KS_HD inline
+#define KS_CE constexpr
 #endif
 
 namespace ksim {
@@ -46,13 +57,14 @@ namespace ksim {
 // TF_HYBRID: the NodePhases block is proven below 2^31 and runs on 32-bit
 // words, the rest on 64-bit words.
 enum : uint32_t { TF_SLOW = 1u, TF_APX = 2u, TF_NARROW = 4u, TF_HYBRID = 8u };
-constexpr int TERM_HDR_BYTES = 48;
+constexpr int TERM_HDR_BYTES = 80;
 constexpr int TERM_APX_BYTES = 16;
 // NodePhases / HalfPi column: W mask words + 1 constant word, padded to 16 B
 KS_HD constexpr int rec1_words(int W) { return (W + 2) & ~1; }
 // PiProducts / PhasePairs column: 2W mask words + 1 constant word, padded
 KS_HD constexpr int rec2_words(int W) { return (2 * W + 2) & ~1; }
-constexpr uint32_t NP_REDUCE_BIT = 8u;
+// lambda^e for |e| <= LAM_MAX; a fast term has max(n1, n3) <= LAM_MAX
+constexpr int LAM_MAX = 127;
 constexpr uint32_t NU_ZERO = 15u;  // PhasePairs factor is exactly zero
 
 // Coefficients as unsigned words, so every add and multiply wraps like the
@@ -239,8 +251,12 @@ struct TermHdr {
     uint32_t pf_idx, flags;
     int32_t power2;
     Zu ff;
-    uint32_t np_sched[4];  // NodePhases schedule per class in run order j = 0, 2, 1, 3
+    uint32_t n_cls[4];  // NodePhases columns per rotation class, in run order j = 0, 2, 1, 3
+    int32_t np_pw;      // halvings of the NodePhases block (a term that survives it)
 };
+// The NodePhases constant C (4 x 64-bit words, mod 2^64) follows the header
+// fields at this offset.
+constexpr int TERM_NPC_OFF = 48;
 
 // The parameter vector's top bit (bit 63 of word W-1) is the constant 1; a
 // column mask that includes it has its constant folded into its parity.
@@ -262,8 +278,80 @@ KS_HD TermHdr load_hdr(const uint8_t *p)
     const int32_t *ff = (const int32_t *)(p + 16);
     h.ff.a = (uint64_t)(int64_t)ff[0]; h.ff.b = (uint64_t)(int64_t)ff[1];
     h.ff.c = (uint64_t)(int64_t)ff[2]; h.ff.d = (uint64_t)(int64_t)ff[3];
-    h.np_sched[0] = u[8]; h.np_sched[1] = u[9]; h.np_sched[2] = u[10]; h.np_sched[3] = u[11];
+    h.n_cls[0] = u[8] & 0xFFFFu; h.n_cls[1] = u[8] >> 16;
+    h.n_cls[2] = u[9] & 0xFFFFu; h.n_cls[3] = u[9] >> 16;
+    h.np_pw = (int32_t)u[10];
     return h;
+}
+
+// ---- powers of lambda = 1 + sqrt2 = (1, 1, 0, 1), a unit of Z[w] ----------
+// lambda^-1 = sqrt2 - 1 = (-1, 1, 0, 1).  Entry e + LAM_MAX holds lambda^e
+// mod 2^64 (the low halves are lambda^e mod 2^32).
+struct LamTable { uint64_t z[2 * LAM_MAX + 1][4]; };
+struct alignas(16) LamTable32 { uint32_t z[2 * LAM_MAX + 1][4]; };
+
+KS_CE void lam_step(uint64_t (&z)[4], const uint64_t (&y)[4])
+{
+    const uint64_t a = z[0] * y[0] + z[1] * y[3] - z[2] * y[2] + z[3] * y[1];
+    const uint64_t b = z[0] * y[1] + z[1] * y[0] + z[2] * y[3] + z[3] * y[2];
+    const uint64_t c = z[0] * y[2] + z[1] * y[1] + z[2] * y[0] - z[3] * y[3];
+    const uint64_t d = z[0] * y[3] - z[1] * y[2] - z[2] * y[1] + z[3] * y[0];
+    z[0] = a; z[1] = b; z[2] = c; z[3] = d;
+}
+
+KS_CE LamTable make_lam_table()
+{
+    LamTable t{};
+    const uint64_t up[4] = {1, 1, 0, 1}, dn[4] = {~0ull, 1, 0, 1};
+    uint64_t p[4] = {1, 0, 0, 0}, n[4] = {1, 0, 0, 0};
+    for (int k = 0; k < 4; ++k) t.z[LAM_MAX][k] = p[k];
+    for (int e = 1; e <= LAM_MAX; ++e) {
+        lam_step(p, up);
+        lam_step(n, dn);
+        for (int k = 0; k < 4; ++k) {
+            t.z[LAM_MAX + e][k] = p[k];
+            t.z[LAM_MAX - e][k] = n[k];
+        }
+    }
+    return t;
+}
+
+KS_CE LamTable32 make_lam_table32()
+{
+    const LamTable t = make_lam_table();
+    LamTable32 r{};
+    for (int e = 0; e < 2 * LAM_MAX + 1; ++e)
+        for (int k = 0; k < 4; ++k) r.z[e][k] = (uint32_t)t.z[e][k];
+    return r;
+}
+
+#if defined(__CUDACC__)
+static __device__ const LamTable kLamDev = make_lam_table();
+static __device__ const LamTable32 kLam32Dev = make_lam_table32();
+#endif
+static constexpr LamTable kLamHost = make_lam_table();
+
+// lambda^e, |e| <= LAM_MAX, in the word type of the path.
+KS_HD Zr<uint64_t> lam_pow(int e, uint64_t)
+{
+#if defined(__CUDA_ARCH__)
+    const ulonglong2 *q = (const ulonglong2 *)&kLamDev.z[e + LAM_MAX][0];
+    const ulonglong2 x = __ldg(q), y = __ldg(q + 1);
+    return {x.x, x.y, y.x, y.y};
+#else
+    const uint64_t *z = kLamHost.z[e + LAM_MAX];
+    return {z[0], z[1], z[2], z[3]};
+#endif
+}
+KS_HD Zr<uint32_t> lam_pow(int e, uint32_t)
+{
+#if defined(__CUDA_ARCH__)
+    const uint4 x = __ldg((const uint4 *)&kLam32Dev.z[e + LAM_MAX][0]);
+    return {x.x, x.y, x.z, x.w};
+#else
+    const uint64_t *z = kLamHost.z[e + LAM_MAX];
+    return {(uint32_t)z[0], (uint32_t)z[1], (uint32_t)z[2], (uint32_t)z[3]};
+#endif
 }
 
 KS_HD int term_bytes(const TermHdr &h, int W)
@@ -316,83 +404,48 @@ KS_HD void ph_update(Zr<T> &z, uint32_t pa, uint32_t pb, uint32_t K)
     }
 }
 
-// One NodePhases column of rotation class J for S shots: factor
-// 1 + (-1)^parity w^J (the mask carries the phase's bit 2 in the constant
-// bit), i.e. z += +-R_J(z); J = 0 is the factor 2 (pw + 1, halved straight
-// back) or 0 (the term dies, pw frozen at the reference's value).
-template <int W, typename T, int S, int J>
-KS_HD const uint64_t *np_column(const uint64_t *q, const uint64_t (&v)[S][W], Zr<T> (&z)[S], int32_t (&pw)[S],
-                                uint32_t (&alive)[S])
+// NodePhases class 0 (factor 1 + s: 2, or 0 when s = -1): a shot whose
+// first (reference order) -1 column is c dies there with the pw the
+// reference had at c, stored in the column word (bits 16..31).
+template <int W, int S>
+KS_HD const uint64_t *np_kill(const uint64_t *q, uint32_t n, const uint64_t (&v)[S][W], uint32_t (&alive)[S],
+                              int32_t (&dead_pw)[S])
 {
     constexpr int R1 = rec1_words(W);
-    uint64_t r[R1];
-    load_rec<R1>(q, r);
-    uint64_t mw[W];
-#pragma unroll
-    for (int w = 0; w < W; ++w) mw[w] = r[w];
-    uint32_t neg[S];
-#pragma unroll
-    for (int s = 0; s < S; ++s) neg[s] = parity<W>(mw, v[s]);
-    if (J == 0) {
-        const int32_t h_before = (int32_t)(((uint32_t)r[W] >> 16) & 0xFFFFu);
+    for (uint32_t t = 0; t < n; ++t, q += R1) {
+        uint64_t r[R1];
+        load_rec<R1>(q, r);
+        const int32_t d = (int32_t)((uint32_t)r[W] >> 16);
 #pragma unroll
         for (int s = 0; s < S; ++s) {
-            pw[s] += (int32_t)(alive[s] & (neg[s] ^ 1u)) + (int32_t)(alive[s] & neg[s]) * h_before;
-            alive[s] &= neg[s] ^ 1u;
-            const T keep = (T)0 - (T)alive[s];
-            z[s].a &= keep; z[s].b &= keep; z[s].c &= keep; z[s].d &= keep;
-        }
-    } else {
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            const Zr<T> t0 = z[s];
-            add_rot(z[s], t0, (uint32_t)J, neg[s]);
+            const uint32_t p = parity<W>(r, v[s]);
+            dead_pw[s] = (alive[s] & p) ? d : dead_pw[s];
+            alive[s] &= p ^ 1u;
         }
     }
-    return q + R1;
+    return q;
 }
 
-template <typename T, int S>
-KS_HD void halve(Zr<T> (&z)[S], int32_t (&pw)[S], const uint32_t (&alive)[S])
+// NodePhases classes 1 to 3: count the columns whose sign is -1.
+template <int W, int S>
+KS_HD const uint64_t *np_count(const uint64_t *q, uint32_t n, const uint64_t (&v)[S][W], uint32_t (&m)[S])
 {
+    constexpr int R1 = rec1_words(W);
+#pragma unroll 2
+    for (uint32_t t = 0; t < n; ++t, q += R1) {
+        uint64_t r[R1];
+        load_rec<R1>(q, r);
 #pragma unroll
-    for (int s = 0; s < S; ++s) {
-        shr_all(z[s], 1u);
-        pw[s] += (int32_t)alive[s];
+        for (int s = 0; s < S; ++s) m[s] += parity<W>(r, v[s]);
     }
-}
-
-// The NodePhases columns of class J (schedule word: see image.cpp): head
-// columns and a halving, k unrolled groups of 4 / nu columns each followed by
-// a halving, then tail columns.
-template <int W, typename T, int S, int J>
-KS_HD const uint64_t *np_class(const uint64_t *q, uint32_t sched, const uint64_t (&v)[S][W], Zr<T> (&z)[S],
-                               int32_t (&pw)[S], uint32_t (&alive)[S])
-{
-    if (J == 0) {
-        for (uint32_t t = 0; t < sched; ++t) q = np_column<W, T, S, 0>(q, v, z, pw, alive);
-        return q;
-    }
-    constexpr int GRP = (J & 1) ? 4 : 2;
-    const uint32_t k = sched & 0xFFFFu, head = (sched >> 16) & 15u, tail = (sched >> 20) & 15u;
-    if (head) {
-        for (uint32_t t = 0; t < head; ++t) q = np_column<W, T, S, J>(q, v, z, pw, alive);
-        halve<T, S>(z, pw, alive);
-    }
-    for (uint32_t g = 0; g < k; ++g) {
-#pragma unroll
-        for (int i = 0; i < GRP; ++i) q = np_column<W, T, S, J>(q, v, z, pw, alive);
-        halve<T, S>(z, pw, alive);
-    }
-    for (uint32_t t = 0; t < tail; ++t) q = np_column<W, T, S, J>(q, v, z, pw, alive);
     return q;
 }
 
 // Fast path: exact when the host proved every coefficient stays below 2^62
 // (T = uint64_t) or that every value it must know exactly stays below 2^31
 // (T = uint32_t, TF_NARROW): adds and multiplies wrap, so intermediate sums
-// may leave the narrow range, but the values at each halving and at the end
-// are the true ones.  S shots at once: each column record is loaded and
+// may leave the narrow range, but the values at each halving, at the
+// widening and at the end are the true ones.  S shots at once: each column record is loaded and
 // decoded once and applied to S independent parameter vectors.
 // TN: word of the NodePhases block, T: word of the rest (TN = uint32_t, T =
 // uint64_t is the hybrid path: NodePhases proven below 2^31, the rest not).
@@ -402,39 +455,44 @@ KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const ui
 {
     constexpr int R1 = rec1_words(W), R2 = rec2_words(W);
     const uint64_t *q = (const uint64_t *)(p + TERM_HDR_BYTES + ((h.flags & TF_APX) ? TERM_APX_BYTES : 0));
-    Zr<TN> zn[S];
+    // NodePhases: sign counts per rotation class (run order j = 0, 2, 1, 3),
+    // then C * lambda^(m3 - m1), rotation w^(6 (m1 + m2 + m3)) deferred
     int32_t pw[S];  // halvings within one term stay far below 2^31
-    uint32_t alive[S];
+    uint32_t alive[S], m1[S], m2[S], m3[S];
 #pragma unroll
     for (int s = 0; s < S; ++s) {
-        zn[s].a = 1; zn[s].b = 0; zn[s].c = 0; zn[s].d = 0;
         pw[s] = 0;
         alive[s] = 1;
+        m1[s] = 0; m2[s] = 0; m3[s] = 0;
     }
-
-    // NodePhases: one branch-free loop per rotation class, in the run order
-    // the host packed (j = 0, 2, 1, 3)
-    q = np_class<W, TN, S, 0>(q, h.np_sched[0], v, zn, pw, alive);
-    q = np_class<W, TN, S, 2>(q, h.np_sched[1], v, zn, pw, alive);
-    q = np_class<W, TN, S, 1>(q, h.np_sched[2], v, zn, pw, alive);
-    q = np_class<W, TN, S, 3>(q, h.np_sched[3], v, zn, pw, alive);
+    q = np_kill<W, S>(q, h.n_cls[0], v, alive, pw);
+    q = np_count<W, S>(q, h.n_cls[1], v, m2);
+    q = np_count<W, S>(q, h.n_cls[2], v, m1);
+    q = np_count<W, S>(q, h.n_cls[3], v, m3);
+    const uint64_t *cp = (const uint64_t *)(p + TERM_NPC_OFF);
+    const Zr<TN> c = {(TN)cp[0], (TN)cp[1], (TN)cp[2], (TN)cp[3]};
+    const bool odd = (h.n_cls[2] | h.n_cls[3]) != 0;
     Zr<T> z[S];
+    uint32_t tot[S];
 #pragma unroll
     for (int s = 0; s < S; ++s) {
+        Zr<TN> zn = c;
+        if (odd) zn = zmul(c, lam_pow((int)m3[s] - (int)m1[s], TN()));
+        const TN keep = (TN)0 - (TN)alive[s];
+        zn.a &= keep; zn.b &= keep; zn.c &= keep; zn.d &= keep;
+        pw[s] = alive[s] ? h.np_pw : pw[s];
+        tot[s] = 6u * (m1[s] + m2[s] + m3[s]);
         if constexpr (sizeof(TN) == sizeof(T)) {
-            z[s].a = (T)zn[s].a; z[s].b = (T)zn[s].b; z[s].c = (T)zn[s].c; z[s].d = (T)zn[s].d;
+            z[s].a = (T)zn.a; z[s].b = (T)zn.b; z[s].c = (T)zn.c; z[s].d = (T)zn.d;
         } else {
-            z[s] = widen(zn[s]);  // sign-extend to the 64-bit words of the rest
+            z[s] = widen(zn);  // sign-extend to the 64-bit words of the rest
         }
     }
     // HalfPi (w^(sum par*coeff)) and PiProducts (a sign, w^4) are units: they
     // change no valuation and commute with the PhasePairs factors, so their
     // rotations are merged with the prefactor's w^idx into one rotation at
     // the end (the reference's renormalisation after HalfPi cannot fire).
-    uint32_t tot[S];
     {
-#pragma unroll
-        for (int s = 0; s < S; ++s) tot[s] = 0;
         for (uint32_t t = 0; t < h.n_hp; ++t, q += R1) {
             uint64_t r[R1];
             load_rec<R1>(q, r);

@@ -181,3 +181,25 @@ def test_valuation_matches_evenness(hostemu):
     # nu(1 - w) = 1, nu(1 + i) = 2, nu(2) = 4, nu(0) = 15 (the zero marker)
     for z, want in (([1, -1, 0, 0], 1), ([1, 0, 1, 0], 2), ([2, 0, 0, 0], 4), ([0, 0, 0, 0], 15)):
         assert hostemu.hostemu_valuation(np.array(z, np.int64).ctypes.data) == want
+
+
+@pytest.mark.parametrize("Tnp", [1, 7, 33, 90])
+def test_nodephases_by_sign_counts(hostemu, oracle_port, Tnp):
+    """NodePhases blocks alone, on every path: the counted form (one constant
+    times lambda^(m3 - m1), rotation w^(6 M), class-0 kill with the
+    reference's pw) gives the reference's per-term numerators, dead terms
+    included."""
+    rng = np.random.default_rng(77 + Tnp)
+    gs = [synth.random_graph(rng, 16, 12 + k, Tnp, 0, 0, 0, density=0.3) for k in range(3)]
+    he = HostEmu(hostemu, gs, 12)
+    po = oracle_port.PortOracle(gs, 12)
+    dead = 0
+    for gi, g in enumerate(gs):
+        P = g.np_params.shape[2]
+        pv = rng.integers(0, 2, size=(64, P)).astype(np.uint8)
+        want = po.eval_terms(gi, pv)
+        assert np.array_equal(he.eval_terms(gi, pv), want), gi
+        assert np.array_equal(he.eval_terms(gi, pv, pairs=True), want), gi
+        dead += int(((want[..., :4] == 0).all(-1) & (want[..., 4] > 0)).sum())
+    if Tnp >= 7:
+        assert dead > 0
