@@ -174,7 +174,9 @@ ksim_status ksim_component_create(const ksim_graph_desc *graphs, int32_t n_graph
     const int64_t slot = std::max<int64_t>(16384, (c->img.max_term_bytes + 15) & ~int64_t(15));
     c->cfg.threads = 256;
     c->cfg.slot_bytes = (int)std::min<int64_t>(slot, 1 << 30);
-    c->cfg.staged = staged_smem_bytes((int)std::min<int64_t>(slot, 1 << 20)) <= 200 * 1024 ? 1 : 0;
+    c->cfg.staged =
+        sample_smem_bytes((int)std::min<int64_t>(slot, 1 << 20), true, c->img.W, c->cfg.threads) <= 200 * 1024 ? 1
+                                                                                                            : 0;
     // free the packed bytes; term offsets stay for re-chunking
     c->img.bytes.clear();
     c->img.bytes.shrink_to_fit();
@@ -221,8 +223,9 @@ ksim_status ksim_component_set_launch(ksim_component *c, int32_t threads, int32_
                             std::to_string(c->img.max_term_bytes) + " bytes)");
         cfg.slot_bytes = slot_bytes;
     }
-    if (cfg.staged && staged_smem_bytes(cfg.slot_bytes) > 227 * 1024)
-        return fail(KSIM_ERR_INVALID_ARGUMENT, "two staging slots exceed 227 KiB of shared memory");
+    if (sample_smem_bytes(cfg.slot_bytes, cfg.staged != 0, c->img.W, cfg.threads) > 227 * 1024)
+        return fail(KSIM_ERR_INVALID_ARGUMENT,
+                    "the staging slots and the parity scratch exceed 227 KiB of shared memory");
     c->cfg = cfg;
     return KSIM_OK;
 }

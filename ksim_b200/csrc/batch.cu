@@ -40,6 +40,12 @@ struct BatchItem {
 
 namespace {
 
+// Class 0 runs W <= 4, class 1 the wider vectors (scratch sized for W = 16).
+size_t batch_smem_bytes(int slot_bytes, int cls, int threads)
+{
+    return sample_smem_bytes(slot_bytes, true, cls == 0 ? 4 : 16, threads);
+}
+
 template <int CLASS>
 __global__ void __launch_bounds__(256, CLASS == 0 ? KSIM_SAMPLE_MIN_CTAS : 1) k_batch(const BatchJobDev *__restrict__ jobs,
                                                const BatchItem *__restrict__ items, int n_items, int *counter)
@@ -50,6 +56,7 @@ __global__ void __launch_bounds__(256, CLASS == 0 ? KSIM_SAMPLE_MIN_CTAS : 1) k_
     uint8_t *slots = smem + BAR_BYTES;
     ring_init(bar);
     uint32_t g = 0;
+    uint8_t *scratch = slots + (size_t)NSLOT * jobs[0].j.slot_bytes;
     for (;;) {
         if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
         __syncthreads();
@@ -61,19 +68,19 @@ __global__ void __launch_bounds__(256, CLASS == 0 ? KSIM_SAMPLE_MIN_CTAS : 1) k_
         bool ok = true;
         if (CLASS == 0) {
             switch (J.W) {
-            case 1: ok = sample_tile<1, true, false, shots_per_thread(1)>(J.j, w.s0, bar, slots, g); break;
-            case 2: ok = sample_tile<2, true, false, shots_per_thread(2)>(J.j, w.s0, bar, slots, g); break;
-            case 3: ok = sample_tile<3, true, false, shots_per_thread(3)>(J.j, w.s0, bar, slots, g); break;
-            default: ok = sample_tile<4, true, false, shots_per_thread(4)>(J.j, w.s0, bar, slots, g); break;
+            case 1: ok = sample_tile<1, true, false, shots_per_thread(1)>(J.j, w.s0, bar, slots, g, scratch); break;
+            case 2: ok = sample_tile<2, true, false, shots_per_thread(2)>(J.j, w.s0, bar, slots, g, scratch); break;
+            case 3: ok = sample_tile<3, true, false, shots_per_thread(3)>(J.j, w.s0, bar, slots, g, scratch); break;
+            default: ok = sample_tile<4, true, false, shots_per_thread(4)>(J.j, w.s0, bar, slots, g, scratch); break;
             }
         } else {
             switch (J.W) {
-            case 5: ok = sample_tile<5, true, false, shots_per_thread(5)>(J.j, w.s0, bar, slots, g); break;
-            case 6: ok = sample_tile<6, true, false, shots_per_thread(6)>(J.j, w.s0, bar, slots, g); break;
-            case 8: ok = sample_tile<8, true, false, shots_per_thread(8)>(J.j, w.s0, bar, slots, g); break;
-            case 10: ok = sample_tile<10, true, false, shots_per_thread(10)>(J.j, w.s0, bar, slots, g); break;
-            case 12: ok = sample_tile<12, true, false, shots_per_thread(12)>(J.j, w.s0, bar, slots, g); break;
-            default: ok = sample_tile<16, true, false, shots_per_thread(16)>(J.j, w.s0, bar, slots, g); break;
+            case 5: ok = sample_tile<5, true, false, shots_per_thread(5)>(J.j, w.s0, bar, slots, g, scratch); break;
+            case 6: ok = sample_tile<6, true, false, shots_per_thread(6)>(J.j, w.s0, bar, slots, g, scratch); break;
+            case 8: ok = sample_tile<8, true, false, shots_per_thread(8)>(J.j, w.s0, bar, slots, g, scratch); break;
+            case 10: ok = sample_tile<10, true, false, shots_per_thread(10)>(J.j, w.s0, bar, slots, g, scratch); break;
+            case 12: ok = sample_tile<12, true, false, shots_per_thread(12)>(J.j, w.s0, bar, slots, g, scratch); break;
+            default: ok = sample_tile<16, true, false, shots_per_thread(16)>(J.j, w.s0, bar, slots, g, scratch); break;
             }
         }
         if (!ok) break;
@@ -105,9 +112,9 @@ static ksim_status batch_enqueue(ksim_batch *b, cudaStream_t st)
 {
     cudaError_t e = cudaMemsetAsync(b->d_counter, 0, 2 * sizeof(int), st);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(work counter)");
-    const size_t smem = staged_smem_bytes(b->slot_bytes);
     for (int cls = 0; cls < 2; ++cls) {
         if (!b->n_items[cls]) continue;
+        const size_t smem = batch_smem_bytes(b->slot_bytes, cls, b->threads);
         if (cls == 0)
             k_batch<0><<<b->grid[0], b->threads, smem, st>>>(b->d_jobs, b->d_items[0], b->n_items[0], b->d_counter);
         else
@@ -136,8 +143,9 @@ ksim_status ksim_batch_create(const ksim_batch_job *jobs, int32_t n_jobs, const 
     }
     if (b->threads > 256 || (b->threads & 31))
         return fail(KSIM_ERR_INVALID_ARGUMENT, "threads must be a multiple of 32 in [32, 256]");
-    if ((b->slot_bytes & 15) || staged_smem_bytes(b->slot_bytes) > 227 * 1024)
-        return fail(KSIM_ERR_INVALID_ARGUMENT, "slot_bytes must be a multiple of 16 and two slots fit in 227 KiB");
+    if ((b->slot_bytes & 15) || batch_smem_bytes(b->slot_bytes, 0, b->threads) > 227 * 1024)
+        return fail(KSIM_ERR_INVALID_ARGUMENT,
+                    "slot_bytes must be a multiple of 16, and two slots with the parity scratch fit in 227 KiB");
     int device = -1;
     for (int i = 0; i < n_jobs; ++i) {
         const ksim_batch_job &jb = jobs[i];
@@ -212,8 +220,8 @@ ksim_status ksim_batch_create(const ksim_batch_job *jobs, int32_t n_jobs, const 
     }
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    const size_t smem = staged_smem_bytes(b->slot_bytes);
     for (int cls = 0; cls < 2; ++cls) {
+        const size_t smem = batch_smem_bytes(b->slot_bytes, cls, b->threads);
         std::vector<int> order(items[cls].size());
         std::iota(order.begin(), order.end(), 0);
         std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[cls][x] > cost[cls][y]; });

@@ -3,16 +3,19 @@
 // Input: the reference's per-graph arrays (sampler.py:21-43 dict layout,
 // kokkos_sim.cpp:91-129 field set).  Output: one byte image
 //   [GraphDir x n_graphs][term stream of graph 0][term stream of graph 1]...
-// Each term record (16-byte aligned), an 80-byte header:
+// Each term record (16-byte aligned) starts with a 96-byte header:
 //   u32 n_np | n_hp<<16, u32 n_pp | n_ph<<16, u32 pf_idx | flags<<16,
 //   i32 power2, i32 floatfactor[4], u32 n0 | n2<<16, u32 n1 | n3<<16 (the
 //   NodePhases columns per rotation class), i32 H (the block's halvings),
-//   u32 0, u64 C[4] (the block's all-plus product / 2^H, mod 2^64),
-//   then [f64 approx re, im], then the columns.
-// Column records hold the parameter masks as W 64-bit words (bit j = param j;
-// the top bit of word W-1 is the constant 1 of the parameter vector, set in a
-// mask when the column's constant is 1) and one constant word:
-//   NodePhases  [mask W][phase | dead_pw<<16]                (count = np_counts[g])
+//   u32 record bytes, u64 C[4] (the block's all-plus product / 2^H, mod
+//   2^64), u32 nb (parity blocks), u32 0, u64 0,
+// then [f64 approx re, im], then the body.  A fast term's body is its parity
+// rows (layout: zring.cuh).  An exact (TF_SLOW) term's body is the columns
+// in the reference's order, each the parameter masks as W 64-bit words (bit j
+// = param j; the top bit of word W-1 is the constant 1 of the parameter
+// vector, set in a mask when the column's constant is 1) and one constant
+// word:
+//   NodePhases  [mask W][phase]                              (count = np_counts[g])
 //   HalfPi      [mask W][coeff & 7]                          (zero coeffs dropped)
 //   PiProducts  [psi W][phi W][psi_c | phi_c<<1]             (identically-zero dropped)
 //   PhasePairs  [alpha W][beta W][ja | K<<2 | jb<<3 | jg<<5] (count = ph_counts[g])
@@ -261,7 +264,9 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 err = gname + ": term " + std::to_string(t) + " count exceeds the padded width";
                 return KSIM_ERR_MALFORMED_PROGRAM;
             }
-            std::vector<uint8_t> rec;  // column records of this term
+            std::vector<uint8_t> rec;  // column records of this term (exact path)
+            struct Row { std::vector<uint64_t> m; uint32_t c; };
+            std::vector<Row> hp_rows, pair_rows, ph_rows;  // parity rows (fast paths)
             double L = 0;              // log2 bound on max_k |sigma_k(z)| (z starts at 1)
             double Lmax = 0;
             const double kLim = 62.0 - 1e-9;
@@ -359,6 +364,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 }
                 const uint32_t coeff = g.hp_coeffs[ci] & 7u;
                 if (coeff == 0 || all_zero(mask.data(), W)) continue;
+                hp_rows.push_back({std::vector<uint64_t>(mask.begin(), mask.begin() + W), coeff});
                 for (int w = 0; w < W; ++w) put64(rec, mask[w]);
                 put64(rec, coeff);
                 for (int w = W + 1; w < R1; ++w) put64(rec, 0);
@@ -380,6 +386,8 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 // constants folded into the parities: psi = parity(psi mask), phi likewise
                 if (pc) mask[W - 1] |= one_bit;
                 if (qc) mask[2 * W - 1] |= one_bit;
+                pair_rows.push_back({std::vector<uint64_t>(mask.begin(), mask.begin() + W), 0});
+                pair_rows.push_back({std::vector<uint64_t>(mask.begin() + W, mask.begin() + 2 * W), 0});
                 for (int w = 0; w < 2 * W; ++w) put64(rec, mask[w]);
                 put64(rec, pc | (qc << 1));
                 for (int w = 2 * W + 1; w < R2; ++w) put64(rec, 0);
@@ -412,6 +420,8 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 step(L + 2.0);  // partial sums of four rotated copies
                 L += fmax > 0 ? std::log2(fmax) + 1e-12 : 0.0;
                 step(L);
+                ph_rows.push_back({std::vector<uint64_t>(mask.begin(), mask.begin() + W), (uint32_t)cw});
+                ph_rows.push_back({std::vector<uint64_t>(mask.begin() + W, mask.begin() + 2 * W), 0});
                 for (int w = 0; w < 2 * W; ++w) put64(rec, mask[w]);
                 put64(rec, cw);
                 for (int w = 2 * W + 1; w < R2; ++w) put64(rec, 0);
@@ -436,27 +446,106 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             for (uint32_t d : dead_pw) max_dead = std::max(max_dead, d);
             if (std::max(n_cls[1], n_cls[3]) > LAM_MAX || !c_ok || max_dead > 0xFFFFu) unsafe = true;
             uint32_t flags = unsafe ? TF_SLOW : (Lmax <= 30.5 ? TF_NARROW : (Lmax_np <= 30.5 ? TF_HYBRID : 0u));
-            // NodePhases records: class order for the fast paths, the
-            // reference's order for the exact path
-            std::vector<uint8_t> np_rec;
-            for (int r = 0; r < cnp; ++r) {
-                const int c = unsafe ? r : order[r];
-                for (int w = 0; w < W; ++w) put64(np_rec, npc[c].m[w]);
-                put64(np_rec, (uint64_t)npc[c].phase | (unsafe ? 0ull : (uint64_t)dead_pw[c] << 16));
-                for (int w = W + 1; w < R1; ++w) put64(np_rec, 0);
+            // the fast paths' parity rows (row order and block masks:
+            // zring.cuh); more than NB_MAX blocks of them sends the term to
+            // the exact path
+            enum : uint32_t { R_P1 = 1, R_P2 = 2, R_P4 = 4, R_E3 = 8, R_E1 = 16, R_PP = 32, R_K0 = 64 };
+            std::vector<const std::vector<uint64_t> *> rows;
+            std::vector<uint32_t> role;  // mask bits of each row
+            const std::vector<uint64_t> zero_row((size_t)W, 0);
+            if (!unsafe) {
+                for (int r = 0; r < cnp; ++r) {
+                    const uint32_t j = npc[order[r]].phase & 3u;
+                    rows.push_back(&npc[order[r]].m);
+                    role.push_back(j == 0 ? R_K0 : (R_P2 | R_P4 | (j == 3 ? R_E3 : j == 1 ? R_E1 : 0u)));
+                }
+                for (const Row &h : hp_rows) {
+                    rows.push_back(&h.m);
+                    role.push_back(((h.c & 1u) ? R_P1 : 0u) | ((h.c & 2u) ? R_P2 : 0u) | ((h.c & 4u) ? R_P4 : 0u));
+                }
+                if (rows.size() & 1u) {
+                    rows.push_back(&zero_row);
+                    role.push_back(0u);
+                }
+                for (size_t i = 0; i < pair_rows.size(); ++i) {
+                    rows.push_back(&pair_rows[i].m);
+                    role.push_back((i & 1u) ? 0u : R_PP);
+                }
+                for (const Row &q : ph_rows) {
+                    rows.push_back(&q.m);
+                    role.push_back(0u);
+                }
+                if (rows.size() > (size_t)32 * NB_MAX) unsafe = true;
             }
+            if (unsafe) flags = TF_SLOW;
             if (g.pf_has_approx) flags |= TF_APX;
+            std::vector<uint8_t> body;  // everything after the header (and approximation)
+            uint32_t nb = 0;
+            if (unsafe) {
+                // the reference's column order and layout
+                for (int c = 0; c < cnp; ++c) {
+                    for (int w = 0; w < W; ++w) put64(body, npc[c].m[w]);
+                    put64(body, (uint64_t)npc[c].phase);
+                    for (int w = W + 1; w < R1; ++w) put64(body, 0);
+                }
+                body.insert(body.end(), rec.begin(), rec.end());
+            } else {
+                for (int r = 0; r < cnp; ++r)
+                    if ((npc[order[r]].phase & 3u) == 0) {
+                        const uint32_t d = dead_pw[order[r]];
+                        body.push_back((uint8_t)(d & 0xFFu));
+                        body.push_back((uint8_t)(d >> 8));
+                    }
+                for (size_t i = 0; i < ph_rows.size(); i += 2) body.push_back((uint8_t)ph_rows[i].c);
+                while (body.size() & 15u) body.push_back(0);
+                nb = (uint32_t)((rows.size() + 31) / 32);
+                const uint16_t zero_off = (uint16_t)(8 * 64 * W);
+                for (uint32_t b = 0; b < nb; ++b) {
+                    std::vector<std::vector<uint16_t>> lists(32);
+                    size_t n_iter = 0;
+                    uint32_t masks[7] = {0, 0, 0, 0, 0, 0, 0};
+                    for (int r = 0; r < 32; ++r) {
+                        const size_t ri = (size_t)b * 32 + (size_t)r;
+                        if (ri >= rows.size()) continue;
+                        for (int k = 0; k < 7; ++k)
+                            if ((role[ri] >> k) & 1u) masks[k] |= 1u << r;
+                        const std::vector<uint64_t> &m = *rows[ri];
+                        for (int w = 0; w < W; ++w)
+                            for (int k = 0; k < 64; ++k)
+                                if ((m[w] >> k) & 1u) lists[r].push_back((uint16_t)(8 * (64 * w + k)));
+                        n_iter = std::max(n_iter, lists[r].size());
+                    }
+                    put32(body, (uint32_t)n_iter);
+                    for (int k = 0; k < 7; ++k) put32(body, masks[k]);
+                    for (size_t i = 0; i < n_iter; ++i)
+                        for (int r = 0; r < 32; ++r) {
+                            const uint16_t o = i < lists[r].size() ? lists[r][i] : zero_off;
+                            body.push_back((uint8_t)(o & 0xFFu));
+                            body.push_back((uint8_t)(o >> 8));
+                        }
+                }
+            }
+            const int apx_bytes = g.pf_has_approx ? TERM_APX_BYTES : 0;
+            const uint64_t rec_bytes = (uint64_t)TERM_HDR_BYTES + (uint64_t)apx_bytes + body.size();
+            if (rec_bytes > 0xFFFFFFFFull) {
+                err = gname + ": a term record exceeds 4 GiB";
+                return KSIM_ERR_UNSUPPORTED;
+            }
             put32(out, (uint32_t)n_np | ((uint32_t)n_hp << 16));
             put32(out, (uint32_t)n_pp | ((uint32_t)n_ph << 16));
             put32(out, (g.pf_phase_idx[t] & 7u) | (flags << 16));
             put32(out, (uint32_t)g.pf_power2[t]);
             for (int i = 0; i < 4; ++i) put32(out, (uint32_t)ff[i]);
-            // NodePhases class counts in run order (j = 0, 2, 1, 3), H and C
+            // NodePhases class counts in run order (j = 0, 2, 1, 3), H, the
+            // record size and C
             put32(out, (uint32_t)n_cls[0] | ((uint32_t)n_cls[2] << 16));
             put32(out, (uint32_t)n_cls[1] | ((uint32_t)n_cls[3] << 16));
             put32(out, unsafe ? 0u : (uint32_t)np_halvings);
-            put32(out, 0u);
+            put32(out, (uint32_t)rec_bytes);
             for (int k = 0; k < 4; ++k) put64(out, unsafe ? 0ull : (uint64_t)C[k]);
+            put32(out, nb);
+            put32(out, 0u);
+            put64(out, 0u);
             if (g.pf_has_approx) {
                 double ar = g.pf_approx_f32[2 * (size_t)t], ai = g.pf_approx_f32[2 * (size_t)t + 1];
                 uint64_t u;
@@ -465,8 +554,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 std::memcpy(&u, &ai, 8);
                 put64(out, u);
             }
-            out.insert(out.end(), np_rec.begin(), np_rec.end());
-            out.insert(out.end(), rec.begin(), rec.end());
+            out.insert(out.end(), body.begin(), body.end());
             (void)ff64;
             const int64_t tb = (int64_t)out.size() - start;
             img.max_term_bytes = std::max(img.max_term_bytes, tb);

@@ -22,6 +22,17 @@ namespace ksim {
 
 __host__ __device__ constexpr int shots_per_thread(int W) { return W <= 4 ? KSIM_SHOTS_PER_THREAD : 1; }
 
+// Shared memory of the warp-sliced parity rows (sample_tile.cuh): per warp one
+// ballot word per parameter bit plus two zero words, per thread and shot
+// ROW_WORDS row-parity words (the blocks of one term and one spare).
+constexpr int ROW_WORDS = 9;
+__host__ __device__ constexpr int ballot_words_per_warp(int W) { return 64 * W + 2; }
+__host__ __device__ constexpr size_t sliced_smem_bytes(int W, int threads)
+{
+    return (size_t)(threads / 32) * (size_t)ballot_words_per_warp(W) * 8u +
+           (size_t)ROW_WORDS * (size_t)shots_per_thread(W) * (size_t)threads * 4u;
+}
+
 // One sampling job: a component image, its input rows and output placement.
 struct SampleJob {
     const uint8_t *image;      // device program image
@@ -77,7 +88,14 @@ cudaError_t launch_noise(const ksim_noise *n, int64_t B, int64_t shot_offset, ui
 
 int noise_device(const ksim_noise *n);
 
-// Shared-memory bytes the staged sampler needs for a slot size.
+// Shared-memory bytes of the staging ring (barriers + two slots).
 size_t staged_smem_bytes(int slot_bytes);
+
+// Shared-memory bytes of a sampling CTA: barriers, the staging slots when
+// staged, then the sliced-parity scratch for W-word vectors.
+inline size_t sample_smem_bytes(int slot_bytes, bool staged, int W, int threads)
+{
+    return (staged ? staged_smem_bytes(slot_bytes) : (size_t)128) + sliced_smem_bytes(W, threads);
+}
 
 }  // namespace ksim

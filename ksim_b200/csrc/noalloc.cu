@@ -58,7 +58,8 @@ __global__ void __launch_bounds__(256, KSIM_SAMPLE_MIN_CTAS) k_sample_noalloc(co
     if (STAGED) ring_init(bar);
     uint32_t g = 0;
     constexpr int S = shots_per_thread(W);
-    sample_tile<W, STAGED, false, S>(j, (int64_t)blockIdx.x * blockDim.x * S, bar, slots, g);
+    uint8_t *scratch = STAGED ? slots + (size_t)NSLOT * j.slot_bytes : slots;
+    sample_tile<W, STAGED, false, S>(j, (int64_t)blockIdx.x * blockDim.x * S, bar, slots, g, scratch);
 }
 
 // Set-up, once per device, with that device current.
@@ -120,14 +121,17 @@ cudaError_t launch_noalloc_w(const SampleJob &j, const LaunchCfg &cfg, cudaStrea
     const int64_t tile = (int64_t)cfg.threads * shots_per_thread(W);
     const int64_t blocks = (j.B + tile - 1) / tile;
     if (blocks > 0x7FFFFFFF) return cudaErrorInvalidConfiguration;
+    const size_t smem = sample_smem_bytes(j.slot_bytes, cfg.staged != 0, W, cfg.threads);
     if (cfg.staged) {
-        const size_t smem = staged_smem_bytes(j.slot_bytes);
         cudaError_t e = cudaFuncSetAttribute(k_sample_noalloc<W, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return e;
         k_sample_noalloc<W, true><<<(unsigned)blocks, cfg.threads, smem, st>>>(j);
     } else {
-        k_sample_noalloc<W, false><<<(unsigned)blocks, cfg.threads, 0, st>>>(j);
+        cudaError_t e = cudaFuncSetAttribute(k_sample_noalloc<W, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        k_sample_noalloc<W, false><<<(unsigned)blocks, cfg.threads, smem, st>>>(j);
     }
     return cudaGetLastError();
 }

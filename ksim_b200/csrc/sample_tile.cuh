@@ -8,9 +8,17 @@
 // chunk by chunk (whole terms, <= slot bytes) from HBM into a two-slot
 // shared-memory ring with TMA bulk copies (cp.async.bulk + mbarrier
 // complete_tx); the copy of chunk c+2 is in flight while chunk c+1 is
-// evaluated, and each warp reads a column record with one broadcast 16-byte
-// shared load.  The shot's parameter vector [f | m | trying] is W 64-bit
-// registers; a parity is AND + popcount.
+// evaluated.  The shot's parameter vector [f | m | trying] is W 64-bit
+// registers.
+//
+// Parities are computed warp-sliced.  Each warp keeps, in shared memory, one
+// 64-bit ballot word per parameter bit (bit s = that bit of the warp's shot
+// s; shots 0-31 are the lanes' first shots, 32-63 their second); a parity
+// row is the XOR of the ballot words of its few set bits, so lane l builds
+// row 32b + l of a block for all 64 shots with a handful of loads, and a
+// 32x32 bit transpose over the warp (five shuffle rounds) gives every shot
+// its 32 row parities as one word.  The term arithmetic then reads
+// row-parity bit ranges (zring.cuh, eval_term_rows).
 //
 // Every mbarrier wait is bounded.  A wait that runs out raises
 // KSIM_FLAG_WAIT_TIMEOUT; the CTA then waits (bounded again) for the copies it
@@ -31,6 +39,7 @@ namespace ksim {
 
 constexpr int NSLOT = 2;
 constexpr int BAR_BYTES = 128;
+static_assert(ROW_WORDS == NB_MAX + 1, "row-parity words per shot: one term's blocks and a spare");
 constexpr long long WAIT_LIMIT = 1ll << 22;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -139,6 +148,117 @@ __device__ __forceinline__ uint32_t get_bit(const uint64_t (&v)[W], int pos)
     return x != 0 ? 1u : 0u;
 }
 
+// 32x32 bit transposes across the warp, two at once: lane i holds row i of
+// each (bit b = column b) and gets column i back (bit b = row b).  Round j
+// swaps the off-diagonal j x j blocks of lane pairs (i, i ^ j).
+__device__ __forceinline__ void transpose32x2(uint32_t &x0, uint32_t &x1, int lane)
+{
+#pragma unroll
+    for (int j = 16; j >= 1; j >>= 1) {
+        const uint32_t m = j == 16 ? 0xFFFF0000u : j == 8 ? 0xFF00FF00u : j == 4 ? 0xF0F0F0F0u
+                         : j == 2 ? 0xCCCCCCCCu : 0xAAAAAAAAu;  // bits b with b & j
+        const bool up = (lane & j) != 0;
+        const uint32_t keep = up ? m : ~m;
+        const uint32_t sh = up ? (uint32_t)j : (uint32_t)(32 - j);  // rotate right by j, or left by j
+        const uint32_t y0 = __shfl_xor_sync(~0u, x0, j);
+        const uint32_t y1 = __shfl_xor_sync(~0u, x1, j);
+        x0 = (x0 & keep) | (__funnelshift_r(y0, y0, sh) & ~keep);
+        x1 = (x1 & keep) | (__funnelshift_r(y1, y1, sh) & ~keep);
+    }
+}
+
+__device__ __forceinline__ uint32_t transpose32(uint32_t x0, int lane)
+{
+#pragma unroll
+    for (int j = 16; j >= 1; j >>= 1) {
+        const uint32_t m = j == 16 ? 0xFFFF0000u : j == 8 ? 0xFF00FF00u : j == 4 ? 0xF0F0F0F0u
+                         : j == 2 ? 0xCCCCCCCCu : 0xAAAAAAAAu;
+        const bool up = (lane & j) != 0;
+        const uint32_t keep = up ? m : ~m;
+        const uint32_t sh = up ? (uint32_t)j : (uint32_t)(32 - j);
+        const uint32_t y0 = __shfl_xor_sync(~0u, x0, j);
+        x0 = (x0 & keep) | (__funnelshift_r(y0, y0, sh) & ~keep);
+    }
+    return x0;
+}
+
+// Ballot words of parameter bits [k0, k1) (warp-uniform bounds).
+template <int W, int S>
+__device__ __forceinline__ void ballot_words(uint64_t *sw, const uint64_t (&vk)[S][W], int k0, int k1, int lane)
+{
+    for (int k = k0; k < k1; ++k) {
+        uint64_t x = __ballot_sync(~0u, get_bit<W>(vk[0], k));
+        if (S > 1) x |= (uint64_t)__ballot_sync(~0u, get_bit<W>(vk[S - 1], k)) << 32;
+        if (lane == (k & 31)) sw[k] = x;
+    }
+    __syncwarp();
+}
+
+// The exact path out of line: rare, and inlined it would take registers from
+// the fast path of every term.
+template <int W>
+__device__ __noinline__ void eval_term_exact_call(const uint8_t *p, const TermHdr &h, const uint64_t (&v)[W],
+                                                  TermOut &o)
+{
+    eval_term_exact<W>(p, h, v, o);
+}
+
+// Terms of one chunk for the warp's shots, adding each term's complex value
+// to (sum_re[s], sum_im[s]) in order (the warp-sliced form of eval_terms_s).
+// sw: the warp's ballot words; wb: this thread's row-parity words (block b,
+// shot r at wb[b * S * blockDim + r * blockDim]).
+template <int W, int S>
+__device__ __forceinline__ const uint8_t *eval_terms_warp(const uint8_t *p, uint32_t n_terms,
+                                                          const uint64_t (&v)[S][W], const uint8_t *sw,
+                                                          uint32_t *wb, double (&sum_re)[S], double (&sum_im)[S],
+                                                          uint32_t &risk, uint32_t live, int lane)
+{
+    const int nt = (int)blockDim.x, wstride = S * nt;
+    for (uint32_t t = 0; t < n_terms; ++t) {
+        const TermHdr h = load_hdr(p);
+        TermOut o[S];
+        if (h.flags & TF_SLOW) {
+#pragma unroll
+            for (int s = 0; s < S; ++s) eval_term_exact_call<W>(p, h, v[s], o[s]);
+        } else {
+            const uint8_t *blk = p + term_blocks_off(h);
+            for (uint32_t b = 0; b < h.nb; ++b) {
+                const uint32_t n_iter = *(const uint32_t *)blk;
+                const uint16_t *ix = (const uint16_t *)(blk + BLOCK_HEAD_BYTES) + lane;
+                uint64_t acc = 0;
+#pragma unroll 4
+                for (uint32_t i = 0; i < n_iter; ++i) acc ^= *(const uint64_t *)(sw + ix[32 * i]);
+                if (S > 1) {
+                    uint32_t x0 = (uint32_t)acc, x1 = (uint32_t)(acc >> 32);
+                    transpose32x2(x0, x1, lane);
+                    wb[b * wstride] = x0;
+                    wb[b * wstride + nt] = x1;
+                } else {
+                    wb[b * wstride] = transpose32((uint32_t)acc, lane);
+                }
+                blk += BLOCK_HEAD_BYTES + 64 * n_iter;
+            }
+            RowBits bits[S];
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                bits[s].w = wb + s * nt;
+                bits[s].stride = wstride;
+            }
+            eval_term_rows_any<S>(p, h, bits, o);
+        }
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            double re, im;
+            term_complex(o[s], p, h.flags, re, im);
+            sum_re[s] = dadd(sum_re[s], re);
+            sum_im[s] = dadd(sum_im[s], im);
+            risk |= o[s].risk & (live >> s);
+        }
+        p += h.rec_bytes;
+    }
+    return p;
+}
+
 // Parameter vector of graph k: [f | m_0..m_{nm-1}] and, for k >= 1, the
 // "trying" bit on every position from F+nm up to the graph's P
 // (kokkos_sim.cpp:10-14 / zx_eval.hpp:86-90), plus the constant-one top bit.
@@ -170,11 +290,14 @@ __device__ __forceinline__ void issue_chunk(const SampleJob &j, int c, uint32_t 
 // Sample shots [s0, s0 + blockDim.x) of job j.  g is the CTA's running chunk
 // count (advanced by the job's chunk count).  Returns false after a wait
 // timeout (the CTA must then stop using the ring).
+// scratch: sliced_smem_bytes(W, blockDim.x) bytes of shared memory.
 template <int W, bool STAGED, bool CG = false, int S = 1>
 __device__ __forceinline__ bool sample_tile(const SampleJob &j, const int64_t s0, uint64_t *bar, uint8_t *slots,
-                                            uint32_t &g)
+                                            uint32_t &g, uint8_t *scratch)
 {
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31;
+    uint64_t *sw = (uint64_t *)scratch + (size_t)(tid >> 5) * ballot_words_per_warp(W);
+    uint32_t *wb = (uint32_t *)(scratch + (size_t)(blockDim.x >> 5) * ballot_words_per_warp(W) * 8) + tid;
     const int F = j.F;
     // thread tid owns shots s0 + tid + r * blockDim.x, r < S
     int64_t sh[S];
@@ -206,11 +329,16 @@ __device__ __forceinline__ bool sample_tile(const SampleJob &j, const int64_t s0
         }
     }
     uint64_t vk[S][W];
-    {
-        const int P0 = graph_params<CG>(j.gdir);
+    int Pk = graph_params<CG>(j.gdir);
 #pragma unroll
-        for (int r = 0; r < S; ++r) graph_vector<W>(vk[r], v[r], F, 0, P0);
+    for (int r = 0; r < S; ++r) graph_vector<W>(vk[r], v[r], F, 0, Pk);
+    ballot_words<W, S>(sw, vk, 0, 64 * W, lane);
+    if (lane == 0) {
+        sw[64 * W] = 0;  // the zero word of short rows
+        sw[64 * W + 1] = 0;
     }
+    __syncwarp();
+    const bool warp_any = __any_sync(~0u, any);
     uint64_t rng[S];
     double prev[S], sre[S], sim[S];
 #pragma unroll
@@ -245,7 +373,8 @@ __device__ __forceinline__ bool sample_tile(const SampleJob &j, const int64_t s0
         } else {
             p = j.image + d.off;
         }
-        if (any) eval_terms_s<W, S>(p, (uint32_t)d.n_terms, vk, sre, sim, risk, live);
+        if (warp_any) eval_terms_warp<W, S>(p, (uint32_t)d.n_terms, vk, (const uint8_t *)sw, wb, sre, sim, risk,
+                                            live, lane);
         if (d.end_of_graph) {
             const int k = d.graph;
 #pragma unroll
@@ -274,9 +403,14 @@ __device__ __forceinline__ bool sample_tile(const SampleJob &j, const int64_t s0
                 sim[r] = 0.0;
             }
             if (k + 1 < j.n_graphs) {
-                const int Pk = graph_params<CG>(j.gdir + k + 1);
+                // bits [F + nm_k, max(P_k, P_k+1)) change: the output just
+                // sampled replaces its trying bit, the trying range follows P
+                const int Pn = graph_params<CG>(j.gdir + k + 1);
 #pragma unroll
-                for (int r = 0; r < S; ++r) graph_vector<W>(vk[r], v[r], F, k + 1, Pk);
+                for (int r = 0; r < S; ++r) graph_vector<W>(vk[r], v[r], F, k + 1, Pn);
+                const int lo = F + (k > 0 ? k - 1 : 0), hi = Pk > Pn ? Pk : Pn;
+                ballot_words<W, S>(sw, vk, lo, hi < 64 * W - 1 ? hi : 64 * W - 1, lane);
+                Pk = Pn;
             }
         }
         if (STAGED) {

@@ -156,12 +156,13 @@ __global__ void __launch_bounds__(256, KSIM_SAMPLE_MIN_CTAS) k_serve(ServeJob *j
         if (slot >= 0) {
             constexpr int S = shots_per_thread(4);  // every loop job has W <= 4
             const int64_t s0 = (int64_t)s_tile * blockDim.x * S;
+            uint8_t *scratch = slots + (size_t)NSLOT * s_job.slot_bytes;
             bool ok;
             switch (s_W) {
-            case 1: ok = sample_tile<1, true, true, S>(s_job, s0, bar, slots, g); break;
-            case 2: ok = sample_tile<2, true, true, S>(s_job, s0, bar, slots, g); break;
-            case 3: ok = sample_tile<3, true, true, S>(s_job, s0, bar, slots, g); break;
-            default: ok = sample_tile<4, true, true, S>(s_job, s0, bar, slots, g); break;
+            case 1: ok = sample_tile<1, true, true, S>(s_job, s0, bar, slots, g, scratch); break;
+            case 2: ok = sample_tile<2, true, true, S>(s_job, s0, bar, slots, g, scratch); break;
+            case 3: ok = sample_tile<3, true, true, S>(s_job, s0, bar, slots, g, scratch); break;
+            default: ok = sample_tile<4, true, true, S>(s_job, s0, bar, slots, g, scratch); break;
             }
             __threadfence();  // this thread's outputs before the counters below
             __syncthreads();
@@ -563,8 +564,9 @@ ksim_status ksim_server_create(const ksim_server_config *cfg_in, ksim_server **o
     if (cfg.idle_us <= 0) cfg.idle_us = 2000;
     if (cfg.threads > 256 || (cfg.threads & 31))
         return fail(KSIM_ERR_INVALID_ARGUMENT, "threads must be a multiple of 32 in [32, 256]");
-    if ((cfg.slot_bytes & 15) || staged_smem_bytes(cfg.slot_bytes) > 227 * 1024)
-        return fail(KSIM_ERR_INVALID_ARGUMENT, "slot_bytes must be a multiple of 16 and two slots fit in 227 KiB");
+    if ((cfg.slot_bytes & 15) || sample_smem_bytes(cfg.slot_bytes, true, 4, cfg.threads) > 227 * 1024)
+        return fail(KSIM_ERR_INVALID_ARGUMENT,
+                    "slot_bytes must be a multiple of 16, and two slots with the parity scratch fit in 227 KiB");
     std::unique_ptr<ksim_server> s(new ksim_server());
     s->device = cfg.device;
     s->cfg = cfg;
@@ -611,7 +613,7 @@ ksim_status ksim_server_create(const ksim_server_config *cfg_in, ksim_server **o
         if ((e = cudaStreamCreateWithFlags(st, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "streams");
     if ((e = cudaEventCreateWithFlags(&s->loop_done, cudaEventDisableTiming)) != cudaSuccess) return bail(e, "events");
     if ((e = cudaEventCreateWithFlags(&s->h2d_mark, cudaEventDisableTiming)) != cudaSuccess) return bail(e, "events");
-    s->smem = staged_smem_bytes(cfg.slot_bytes);
+    s->smem = sample_smem_bytes(cfg.slot_bytes, true, 4, cfg.threads);
     if ((e = cudaFuncSetAttribute(k_serve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem)) != cudaSuccess)
         return bail(e, "loop kernel attributes");
     int active = 0, sms = 0;

@@ -57,7 +57,7 @@ namespace ksim {
 // TF_HYBRID: the NodePhases block is proven below 2^31 and runs on 32-bit
 // words, the rest on 64-bit words.
 enum : uint32_t { TF_SLOW = 1u, TF_APX = 2u, TF_NARROW = 4u, TF_HYBRID = 8u };
-constexpr int TERM_HDR_BYTES = 80;
+constexpr int TERM_HDR_BYTES = 96;
 constexpr int TERM_APX_BYTES = 16;
 // NodePhases / HalfPi column: W mask words + 1 constant word, padded to 16 B
 KS_HD constexpr int rec1_words(int W) { return (W + 2) & ~1; }
@@ -253,10 +253,14 @@ struct TermHdr {
     Zu ff;
     uint32_t n_cls[4];  // NodePhases columns per rotation class, in run order j = 0, 2, 1, 3
     int32_t np_pw;      // halvings of the NodePhases block (a term that survives it)
+    uint32_t rec_bytes; // the whole term record
+    uint32_t nb;          // 32-row parity blocks (fast terms)
 };
 // The NodePhases constant C (4 x 64-bit words, mod 2^64) follows the header
 // fields at this offset.
 constexpr int TERM_NPC_OFF = 48;
+// A fast term has at most this many 32-row parity blocks.
+constexpr int NB_MAX = 8;
 
 // The parameter vector's top bit (bit 63 of word W-1) is the constant 1; a
 // column mask that includes it has its constant folded into its parity.
@@ -281,6 +285,8 @@ KS_HD TermHdr load_hdr(const uint8_t *p)
     h.n_cls[0] = u[8] & 0xFFFFu; h.n_cls[1] = u[8] >> 16;
     h.n_cls[2] = u[9] & 0xFFFFu; h.n_cls[3] = u[9] >> 16;
     h.np_pw = (int32_t)u[10];
+    h.rec_bytes = u[11];
+    h.nb = u[20];
     return h;
 }
 
@@ -354,11 +360,7 @@ KS_HD Zr<uint32_t> lam_pow(int e, uint32_t)
 #endif
 }
 
-KS_HD int term_bytes(const TermHdr &h, int W)
-{
-    return TERM_HDR_BYTES + ((h.flags & TF_APX) ? TERM_APX_BYTES : 0) +
-           8 * (rec1_words(W) * (int)(h.n_np + h.n_hp) + rec2_words(W) * (int)(h.n_pp + h.n_ph));
-}
+KS_HD int term_bytes(const TermHdr &h, int) { return (int)h.rec_bytes; }
 
 // Load R 64-bit words of a 16-byte aligned record with 16-byte vector loads.
 template <int R>
@@ -404,171 +406,199 @@ KS_HD void ph_update(Zr<T> &z, uint32_t pa, uint32_t pb, uint32_t K)
     }
 }
 
-// NodePhases class 0 (factor 1 + s: 2, or 0 when s = -1): a shot whose
-// first (reference order) -1 column is c dies there with the pw the
-// reference had at c, stored in the column word (bits 16..31).
-template <int W, int S>
-KS_HD const uint64_t *np_kill(const uint64_t *q, uint32_t n, const uint64_t (&v)[S][W], uint32_t (&alive)[S],
-                              int32_t (&dead_pw)[S])
+// ---- fast terms: parity rows -------------------------------------------------
+// A fast term's columns are parity rows over the parameter vector, each
+// stored as the list of its set bits.  Row order (term-relative position):
+//   NodePhases class 0, 2, 1, 3 | HalfPi | (a zero row if needed to make the
+//   next position even) | PiProducts (psi, phi) pairs | PhasePairs (alpha,
+//   beta) pairs
+// After the header (and approximation): u16 dead_pw per class-0 row, u8 word
+// (ja | K<<2 | jb<<3 | jg<<5) per PhasePairs column, padded to 16 bytes;
+// then nb blocks of 32 rows, each a 32-byte head
+//   u32 n_iter, u32 masks P1, P2, P4, E3, E1, PP, K0 (bit i = row 32b + i)
+// and n_iter x 32 u16 byte offsets (8 x bit index; entry [i][r] = the i-th
+// set bit of row r of the block, 8 x 64W, the zero word, when it has fewer).
+// Every sum the term needs is linear in the row bits w of a block:
+//   rotation  += popc(w & P1) + 2 popc(w & P2) + 4 popc(w & (P4 | PP & w >> 1))
+//     (P2 and P4 hold the NodePhases classes 1-3, whose sign count enters as
+//     w^6 per -1; P1 / P2 / P4 the HalfPi rows by coefficient bit; PP the psi
+//     rows, whose pair product psi * phi is a sign, w^4)
+//   lambda exponent += popc((w & E3) | (~w & E1)), minus n1 at the end
+//     (= m3 - m1 with E3 / E1 the class-3 / class-1 rows)
+//   kill: the first row of w & K0 (class 0) with its dead_pw.
+constexpr int BLOCK_HEAD_BYTES = 32;
+KS_HD int term_meta_off(const TermHdr &h) { return TERM_HDR_BYTES + ((h.flags & TF_APX) ? TERM_APX_BYTES : 0); }
+KS_HD int term_blocks_off(const TermHdr &h)
 {
-    constexpr int R1 = rec1_words(W);
-    for (uint32_t t = 0; t < n; ++t, q += R1) {
-        uint64_t r[R1];
-        load_rec<R1>(q, r);
-        const int32_t d = (int32_t)((uint32_t)r[W] >> 16);
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            const uint32_t p = parity<W>(r, v[s]);
-            dead_pw[s] = (alive[s] & p) ? d : dead_pw[s];
-            alive[s] &= p ^ 1u;
-        }
-    }
-    return q;
+    return term_meta_off(h) + ((2 * (int)h.n_cls[0] + (int)h.n_ph + 15) & ~15);
+}
+// Position of the first PhasePairs row.
+KS_HD int term_ph_row0(const TermHdr &h)
+{
+    const int pp0 = ((int)(h.n_np + h.n_hp) + 1) & ~1;
+    return pp0 + 2 * (int)h.n_pp;
 }
 
-// NodePhases classes 1 to 3: count the columns whose sign is -1.
-template <int W, int S>
-KS_HD const uint64_t *np_count(const uint64_t *q, uint32_t n, const uint64_t (&v)[S][W], uint32_t (&m)[S])
+KS_HD uint32_t popc32(uint32_t x)
 {
-    constexpr int R1 = rec1_words(W);
-#pragma unroll 2
-    for (uint32_t t = 0; t < n; ++t, q += R1) {
-        uint64_t r[R1];
-        load_rec<R1>(q, r);
+#if defined(__CUDA_ARCH__)
+    return (uint32_t)__popc(x);
+#else
+    return (uint32_t)__builtin_popcount(x);
+#endif
+}
+KS_HD int ffs32(uint32_t x)
+{
+#if defined(__CUDA_ARCH__)
+    return __ffs((int)x) - 1;
+#else
+    return __builtin_ctz(x);
+#endif
+}
+
+// Row-parity words of one shot: word b holds rows 32b..32b+31 (bit i = row
+// 32b + i), `stride` words apart (shared memory, one column per thread) or
+// contiguous (a local array).
+struct RowBits {
+    const uint32_t *w;
+    int stride;
+    KS_HD uint32_t word(int b) const { return w[b * stride]; }
+};
+
+// Parity-row words of one shot from the block records, bit by bit (the
+// per-shot form; the sampling kernels build them for a warp at once).
+template <int W>
+KS_HD void term_words_shot(const uint8_t *p, const TermHdr &h, const uint64_t (&v)[W], uint32_t (&out)[NB_MAX + 1])
+{
+    const uint8_t *blk = p + term_blocks_off(h);
+    for (int b = 0; b <= NB_MAX; ++b) out[b] = 0;
+    for (uint32_t b = 0; b < h.nb; ++b) {
+        const uint32_t n_iter = *(const uint32_t *)blk;
+        const uint16_t *ix = (const uint16_t *)(blk + BLOCK_HEAD_BYTES);
+        uint32_t word = 0;
+        for (int r = 0; r < 32; ++r) {
+            uint32_t par = 0;
+            for (uint32_t i = 0; i < n_iter; ++i) {
+                const uint32_t k = (uint32_t)ix[i * 32 + r] >> 3;
+                uint64_t bit = 0;
 #pragma unroll
-        for (int s = 0; s < S; ++s) m[s] += parity<W>(r, v[s]);
+                for (int w = 0; w < W; ++w) bit |= ((uint32_t)w == (k >> 6)) ? (v[w] >> (k & 63u)) & 1u : 0u;
+                par ^= (uint32_t)bit;
+            }
+            word |= par << r;
+        }
+        out[b] = word;
+        blk += BLOCK_HEAD_BYTES + 64 * n_iter;
     }
-    return q;
 }
 
 // Fast path: exact when the host proved every coefficient stays below 2^62
 // (T = uint64_t) or that every value it must know exactly stays below 2^31
 // (T = uint32_t, TF_NARROW): adds and multiplies wrap, so intermediate sums
 // may leave the narrow range, but the values at each halving, at the
-// widening and at the end are the true ones.  S shots at once: each column record is loaded and
-// decoded once and applied to S independent parameter vectors.
+// widening and at the end are the true ones.  S shots at once, from their
+// parity-row bits.
 // TN: word of the NodePhases block, T: word of the rest (TN = uint32_t, T =
 // uint64_t is the hybrid path: NodePhases proven below 2^31, the rest not).
-template <int W, typename TN, typename T, int S>
-KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const uint64_t (&v)[S][W],
-                                    TermOut (&o)[S])
+template <typename TN, typename T, int S>
+KS_HD const uint8_t *eval_term_rows(const uint8_t *p, const TermHdr &h, const RowBits (&bits)[S], TermOut (&o)[S])
 {
-    constexpr int R1 = rec1_words(W), R2 = rec2_words(W);
-    const uint64_t *q = (const uint64_t *)(p + TERM_HDR_BYTES + ((h.flags & TF_APX) ? TERM_APX_BYTES : 0));
-    // NodePhases: sign counts per rotation class (run order j = 0, 2, 1, 3),
-    // then C * lambda^(m3 - m1), rotation w^(6 (m1 + m2 + m3)) deferred
+    const uint8_t *meta = p + term_meta_off(h);
+    const uint16_t *dead_pw = (const uint16_t *)meta;
+    const uint8_t *ph_cw = meta + 2 * h.n_cls[0];
+    // the block sums: rotation, lambda exponent, class-0 kill
+    uint32_t rot[S], lam[S], alive[S];
     int32_t pw[S];  // halvings within one term stay far below 2^31
-    uint32_t alive[S], m1[S], m2[S], m3[S];
 #pragma unroll
     for (int s = 0; s < S; ++s) {
-        pw[s] = 0;
+        rot[s] = 0;
+        lam[s] = 0;
         alive[s] = 1;
-        m1[s] = 0; m2[s] = 0; m3[s] = 0;
+        pw[s] = h.np_pw;
     }
-    q = np_kill<W, S>(q, h.n_cls[0], v, alive, pw);
-    q = np_count<W, S>(q, h.n_cls[1], v, m2);
-    q = np_count<W, S>(q, h.n_cls[2], v, m1);
-    q = np_count<W, S>(q, h.n_cls[3], v, m3);
+    const uint8_t *blk = p + term_blocks_off(h);
+    for (uint32_t b = 0; b < h.nb; ++b) {
+        const uint32_t *m = (const uint32_t *)blk;
+        const uint32_t P1 = m[1], P2 = m[2], P4 = m[3], E3 = m[4], E1 = m[5], PP = m[6], K0 = m[7];
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const uint32_t w = bits[s].word((int)b);
+            if (K0) {
+                const uint32_t k = w & K0;
+                if (k != 0 && alive[s]) {
+                    pw[s] = (int32_t)dead_pw[32 * b + (uint32_t)ffs32(k)];
+                    alive[s] = 0;
+                }
+            }
+            rot[s] += popc32(w & P1) + 2u * popc32(w & P2) + 4u * popc32(w & (P4 | (PP & (w >> 1))));
+            lam[s] += popc32((w & E3) | (~w & E1));
+        }
+        blk += BLOCK_HEAD_BYTES + 64 * m[0];
+    }
+    // NodePhases: C * lambda^(m3 - m1); its rotation w^(6 (m1 + m2 + m3)) is
+    // in rot with the HalfPi and PiProducts ones (units: they change no
+    // valuation and commute with the PhasePairs factors, so they join the
+    // prefactor's w^idx at the end; the reference's renormalisation after
+    // HalfPi cannot fire)
     const uint64_t *cp = (const uint64_t *)(p + TERM_NPC_OFF);
     const Zr<TN> c = {(TN)cp[0], (TN)cp[1], (TN)cp[2], (TN)cp[3]};
     const bool odd = (h.n_cls[2] | h.n_cls[3]) != 0;
     Zr<T> z[S];
-    uint32_t tot[S];
 #pragma unroll
     for (int s = 0; s < S; ++s) {
         Zr<TN> zn = c;
-        if (odd) zn = zmul(c, lam_pow((int)m3[s] - (int)m1[s], TN()));
+        if (odd) zn = zmul(c, lam_pow((int)lam[s] - (int)h.n_cls[2], TN()));
         const TN keep = (TN)0 - (TN)alive[s];
         zn.a &= keep; zn.b &= keep; zn.c &= keep; zn.d &= keep;
-        pw[s] = alive[s] ? h.np_pw : pw[s];
-        tot[s] = 6u * (m1[s] + m2[s] + m3[s]);
         if constexpr (sizeof(TN) == sizeof(T)) {
             z[s].a = (T)zn.a; z[s].b = (T)zn.b; z[s].c = (T)zn.c; z[s].d = (T)zn.d;
         } else {
             z[s] = widen(zn);  // sign-extend to the 64-bit words of the rest
         }
     }
-    // HalfPi (w^(sum par*coeff)) and PiProducts (a sign, w^4) are units: they
-    // change no valuation and commute with the PhasePairs factors, so their
-    // rotations are merged with the prefactor's w^idx into one rotation at
-    // the end (the reference's renormalisation after HalfPi cannot fire).
-    {
-        for (uint32_t t = 0; t < h.n_hp; ++t, q += R1) {
-            uint64_t r[R1];
-            load_rec<R1>(q, r);
-            uint64_t mw[W];
-#pragma unroll
-            for (int w = 0; w < W; ++w) mw[w] = r[w];
-            const uint32_t coeff = (uint32_t)r[W];
-#pragma unroll
-            for (int s = 0; s < S; ++s) tot[s] += parity<W>(mw, v[s]) ? coeff : 0u;
-        }
-    }
-    // PiProducts: overall sign, kept in tot as w^4
-    {
-        uint32_t e[S];
-#pragma unroll
-        for (int s = 0; s < S; ++s) e[s] = 0;
-        for (uint32_t t = 0; t < h.n_pp; ++t, q += R2) {
-            uint64_t r[R2];
-            load_rec<R2>(q, r);
-            uint64_t ma[W], mb[W];
-#pragma unroll
-            for (int w = 0; w < W; ++w) { ma[w] = r[w]; mb[w] = r[W + w]; }
-#pragma unroll
-            for (int s = 0; s < S; ++s) e[s] ^= parity<W>(ma, v[s]) & parity<W>(mb, v[s]);
-        }
-#pragma unroll
-        for (int s = 0; s < S; ++s) tot[s] += 4u * e[s];
-    }
+    const int ph0 = term_ph_row0(h);
     // PhasePairs: after each factor the reference's renormalisation step,
     // halve once if all four coefficients are even and not all zero
     // (zx_eval.hpp:35-41).  z here differs from the reference's by a unit
-    // (the NodePhases run order, the deferred HalfPi / PiProducts rotation),
-    // and units preserve evenness, so every decision is the reference's.
-    {
-        for (uint32_t t = 0; t < h.n_ph; ++t, q += R2) {
-            uint64_t r[R2];
-            load_rec<R2>(q, r);
-            uint64_t ma[W], mb[W];
+    // (the NodePhases form, the deferred rotations), and units preserve
+    // evenness, so every decision is the reference's.
+    for (uint32_t t = 0; t < h.n_ph; ++t) {
+        const uint32_t cw = ph_cw[t];
+        const uint32_t K = (cw >> 2) & 1u;
+        uint32_t pa[S], pb[S];
 #pragma unroll
-            for (int w = 0; w < W; ++w) { ma[w] = r[w]; mb[w] = r[W + w]; }
-            const uint32_t cw = (uint32_t)r[2 * W];
-            const uint32_t K = (cw >> 2) & 1u;
-            // pa, pb: parities with bit 2 of alpha / beta folded in
-            uint32_t pa[S], pb[S];
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-                pa[s] = parity<W>(ma, v[s]);
-                pb[s] = parity<W>(mb, v[s]);
-            }
-            // one branch on the rotation pair; the third rotation is their sum
-            switch ((cw & 3u) | ((cw >> 1) & 12u)) {
+        for (int s = 0; s < S; ++s) {
+            const int pos = ph0 + 2 * (int)t;
+            const uint32_t x = bits[s].word(pos >> 5) >> (pos & 31);
+            pa[s] = x & 1u;
+            pb[s] = (x >> 1) & 1u;
+        }
+        // one branch on the rotation pair; the third rotation is their sum
+        switch ((cw & 3u) | ((cw >> 1) & 12u)) {
 #define KSIM_PH_CASE(JA, JB)                                                        \
     case (JA) | ((JB) << 2):                                                        \
         _Pragma("unroll") for (int s = 0; s < S; ++s) ph_update<T, JA, JB>(z[s], pa[s], pb[s], K); \
         break;
-            KSIM_PH_CASE(0, 0) KSIM_PH_CASE(1, 0) KSIM_PH_CASE(2, 0) KSIM_PH_CASE(3, 0)
-            KSIM_PH_CASE(0, 1) KSIM_PH_CASE(1, 1) KSIM_PH_CASE(2, 1) KSIM_PH_CASE(3, 1)
-            KSIM_PH_CASE(0, 2) KSIM_PH_CASE(1, 2) KSIM_PH_CASE(2, 2) KSIM_PH_CASE(3, 2)
-            KSIM_PH_CASE(0, 3) KSIM_PH_CASE(1, 3) KSIM_PH_CASE(2, 3) KSIM_PH_CASE(3, 3)
+        KSIM_PH_CASE(0, 0) KSIM_PH_CASE(1, 0) KSIM_PH_CASE(2, 0) KSIM_PH_CASE(3, 0)
+        KSIM_PH_CASE(0, 1) KSIM_PH_CASE(1, 1) KSIM_PH_CASE(2, 1) KSIM_PH_CASE(3, 1)
+        KSIM_PH_CASE(0, 2) KSIM_PH_CASE(1, 2) KSIM_PH_CASE(2, 2) KSIM_PH_CASE(3, 2)
+        KSIM_PH_CASE(0, 3) KSIM_PH_CASE(1, 3) KSIM_PH_CASE(2, 3) KSIM_PH_CASE(3, 3)
 #undef KSIM_PH_CASE
-            }
+        }
 #pragma unroll
-            for (int s = 0; s < S; ++s) {
-                const T o = z[s].a | z[s].b | z[s].c | z[s].d;
-                const uint32_t red = (o != 0 && (o & 1u) == 0) ? 1u : 0u;
-                shr_all(z[s], red);
-                pw[s] += (int32_t)red;
-            }
+        for (int s = 0; s < S; ++s) {
+            const T ov = z[s].a | z[s].b | z[s].c | z[s].d;
+            const uint32_t red = (ov != 0 && (ov & 1u) == 0) ? 1u : 0u;
+            shr_all(z[s], red);
+            pw[s] += (int32_t)red;
         }
     }
-    // prefactor: w^(HalfPi + PiProducts + idx), then the exact floatfactor
-    // with one renormalisation
+    // prefactor: w^(NodePhases + HalfPi + PiProducts + idx), then the exact
+    // floatfactor with one renormalisation
     const Zr<T> ff = {(T)h.ff.a, (T)h.ff.b, (T)h.ff.c, (T)h.ff.d};
 #pragma unroll
     for (int s = 0; s < S; ++s) {
-        Zr<T> zz = rot_var(z[s], (tot[s] + h.pf_idx) & 7u);
+        Zr<T> zz = rot_var(z[s], (rot[s] + h.pf_idx) & 7u);
         zz = zmul(zz, ff);
         zreduce(zz, pw[s]);
         if constexpr (sizeof(T) == 8) {
@@ -580,7 +610,17 @@ KS_HD const uint8_t *eval_term_fast(const uint8_t *p, const TermHdr &h, const ui
         o[s].power2 = h.power2;
         o[s].risk = 0;
     }
-    return (const uint8_t *)q;
+    return p + h.rec_bytes;
+}
+
+// A fast term on the path its header selects.
+template <int S>
+KS_HD const uint8_t *eval_term_rows_any(const uint8_t *p, const TermHdr &h, const RowBits (&bits)[S],
+                                        TermOut (&o)[S])
+{
+    if (h.flags & TF_NARROW) return eval_term_rows<uint32_t, uint32_t, S>(p, h, bits, o);
+    if (h.flags & TF_HYBRID) return eval_term_rows<uint32_t, uint64_t, S>(p, h, bits, o);
+    return eval_term_rows<uint64_t, uint64_t, S>(p, h, bits, o);
 }
 
 // Exact path: the reference's step-by-step arithmetic (zx_eval.hpp:101-165),
@@ -665,20 +705,26 @@ KS_HD void term_complex(const TermOut &o, const uint8_t *hdr_ptr, uint32_t flags
     }
 }
 
-// One term for S shots on the path its header selects.  Returns the next record.
+// One term for S shots on the path its header selects (per-shot parity rows).
+// Returns the next record.
 template <int W, int S>
 KS_HD const uint8_t *eval_term_s(const uint8_t *p, const TermHdr &h, const uint64_t (&v)[S][W],
                                  TermOut (&o)[S])
 {
     if (h.flags & TF_SLOW) {
-        const uint8_t *next = p;
 #pragma unroll
-        for (int s = 0; s < S; ++s) next = eval_term_exact<W>(p, h, v[s], o[s]);
-        return next;
+        for (int s = 0; s < S; ++s) eval_term_exact<W>(p, h, v[s], o[s]);
+        return p + h.rec_bytes;
     }
-    if (h.flags & TF_NARROW) return eval_term_fast<W, uint32_t, uint32_t, S>(p, h, v, o);
-    if (h.flags & TF_HYBRID) return eval_term_fast<W, uint32_t, uint64_t, S>(p, h, v, o);
-    return eval_term_fast<W, uint64_t, uint64_t, S>(p, h, v, o);
+    uint32_t words[S][NB_MAX + 1];
+    RowBits bits[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        term_words_shot<W>(p, h, v[s], words[s]);
+        bits[s].w = words[s];
+        bits[s].stride = 1;
+    }
+    return eval_term_rows_any<S>(p, h, bits, o);
 }
 
 // One term for one shot.
