@@ -110,18 +110,20 @@ bool all_zero(const uint64_t *m, int W)
 // formulation the kernels run (the roofline numerator).  c = 1 on 32-bit
 // words (TF_NARROW), 2 on 64-bit words; exact-path terms are costed as the
 // reference's step-by-step arithmetic (one Z[w] product = 16 64-bit
-// multiplies x 3 + 12 64-bit adds x 2 + renormalisation 12 = 84 per factor).
-//   parity of one W-word mask: 3W (and / xor / fold) + 2 (popcount, bit)
-//   NodePhases j != 0: parity + 1 (sign) + 4c (signed adds) [+ 4c + 1 halving]
-//                      (c = 1 also on the hybrid path, TF_HYBRID)
-//   NodePhases j == 0: parity + 2
-//   HalfPi: parity + 1;  PiProducts: 2 parities + 1
-//   PhasePairs: 2 parities + 3 (signs) + 12c (three rotated adds)
-//               + 4 (valuation) + 4c + 1 (conditional halving)
-//   per term: rotations and signs 28c, floatfactor product 28 (c = 1) or
-//             72 (c = 2), renormalisation 6c, complex value and sum 16
-//   per graph: parameter vector 4W + 8, Bernoulli step 10
-double term_work(int W, uint32_t flags, const int n_cls[4], int n_hp, int n_pp, int n_ph)
+// multiplies x 3 + 12 64-bit adds x 2 + renormalisation 12 = 84 per factor,
+// and a parity of a W-word mask 3W + 2).
+//   fast term, per 32-row parity block (64 shots of a warp share it):
+//     row XORs: 32 rows x n_iter x 2 (64-bit xor) / 64 shots = n_iter
+//       (n_iter: index slots per row of the block, even)
+//     transposes: 2 x 5 rounds x 2 (rotate, select) x 32 lanes / 64 = 10
+//     block sums: 4 (and) + 4 (popcount) + 1 (shift) + 4 (accumulate) = 13
+//   NodePhases: C * lambda^e, 16 multiply-adds x c_np + 4 (mask) + 2
+//   PhasePairs: 3 (bits) + 3 (signs) + 12c (three rotated adds)
+//               + 4 (evenness) + 4c + 1 (conditional halving)
+//   per term: ff * w^k read 4, floatfactor product 16 (c = 1) or 64 (c = 2),
+//             renormalisation 6c, complex value and sum 16
+//   per graph: parameter vector 4W + 8, ballot words 4, Bernoulli step 10
+double term_work(int W, uint32_t flags, const int n_cls[4], int n_hp, int n_pp, int n_ph, int nb, int sum_iter)
 {
     const double par = 3.0 * W + 2.0;
     const int n_np = n_cls[0] + n_cls[1] + n_cls[2] + n_cls[3];
@@ -129,18 +131,15 @@ double term_work(int W, uint32_t flags, const int n_cls[4], int n_hp, int n_pp, 
         return 84.0 * (n_np + n_ph + 3) + par * (n_np + n_hp + 2.0 * n_pp + 2.0 * n_ph) + 16.0;
     const double c = (flags & TF_NARROW) ? 1.0 : 2.0;
     const double cn = (flags & (TF_NARROW | TF_HYBRID)) ? 1.0 : 2.0;  // NodePhases words
-    // NodePhases: a parity and a count (class 0: a parity and a kill test)
-    // per column, then C * lambda^e (a table read and a product) per term
-    double w = n_cls[0] * (par + 2.0) + (n_np - n_cls[0]) * (par + 1.0);
+    double w = (double)sum_iter + 23.0 * nb;
     if (n_cls[1] | n_cls[3]) w += 16.0 * cn + 2.0;
-    w += 4.0 * cn + 4.0;
-    w += n_hp * (par + 1.0) + n_pp * (2.0 * par + 1.0);
-    w += n_ph * (2.0 * par + 3.0 + 12.0 * c + 4.0 + 4.0 * c + 1.0);
-    w += 28.0 * c + (c == 1.0 ? 28.0 : 72.0) + 6.0 * c + 16.0;
+    w += 4.0 * cn;
+    w += n_ph * (3.0 + 3.0 + 12.0 * c + 4.0 + 4.0 * c + 1.0);
+    w += 4.0 + (c == 1.0 ? 16.0 : 64.0) + 6.0 * c + 16.0;
     return w;
 }
 
-double graph_work(int W) { return 4.0 * W + 8.0 + 10.0; }
+double graph_work(int W) { return 4.0 * W + 8.0 + 4.0 + 10.0; }
 
 int supported_words(int needed)
 {
@@ -444,7 +443,11 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             // in range whatever the bound)
             uint32_t max_dead = 0;
             for (uint32_t d : dead_pw) max_dead = std::max(max_dead, d);
-            if (std::max(n_cls[1], n_cls[3]) > LAM_MAX || !c_ok || max_dead > 0xFFFFu) unsafe = true;
+            // (the tabulated ff * w^k negates coefficients: INT32_MIN has no
+            // 32-bit negative)
+            bool ff_min = false;
+            for (int i = 0; i < 4; ++i) ff_min |= ff[i] == INT32_MIN;
+            if (std::max(n_cls[1], n_cls[3]) > LAM_MAX || !c_ok || max_dead > 0xFFFFu || ff_min) unsafe = true;
             uint32_t flags = unsafe ? TF_SLOW : (Lmax <= 30.5 ? TF_NARROW : (Lmax_np <= 30.5 ? TF_HYBRID : 0u));
             // the fast paths' parity rows (row order and block masks:
             // zring.cuh); more than NB_MAX blocks of them sends the term to
@@ -480,7 +483,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             if (unsafe) flags = TF_SLOW;
             if (g.pf_has_approx) flags |= TF_APX;
             std::vector<uint8_t> body;  // everything after the header (and approximation)
-            uint32_t nb = 0;
+            uint32_t nb = 0, sum_iter = 0;
             if (unsafe) {
                 // the reference's column order and layout
                 for (int c = 0; c < cnp; ++c) {
@@ -490,6 +493,19 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 }
                 body.insert(body.end(), rec.begin(), rec.end());
             } else {
+                // ff * w^(k + phase index), k = 0..7
+                {
+                    int64_t z[4] = {ff[0], ff[1], ff[2], ff[3]};
+                    for (uint32_t r = 0; r < (g.pf_phase_idx[t] & 7u); ++r) {
+                        const int64_t a = z[0], b = z[1], c = z[2], d = z[3];
+                        z[0] = d; z[1] = a; z[2] = b; z[3] = -c;  // times w
+                    }
+                    for (int k = 0; k < 8; ++k) {
+                        for (int i = 0; i < 4; ++i) put32(body, (uint32_t)(int32_t)z[i]);
+                        const int64_t a = z[0], b = z[1], c = z[2], d = z[3];
+                        z[0] = d; z[1] = a; z[2] = b; z[3] = -c;
+                    }
+                }
                 for (int r = 0; r < cnp; ++r)
                     if ((npc[order[r]].phase & 3u) == 0) {
                         const uint32_t d = dead_pw[order[r]];
@@ -502,7 +518,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 const uint16_t zero_off = (uint16_t)(8 * 64 * W);
                 for (uint32_t b = 0; b < nb; ++b) {
                     std::vector<std::vector<uint16_t>> lists(32);
-                    size_t n_iter = 0;
+                    size_t n_iter = 0;  // index slots per row, rounded up to pairs
                     uint32_t masks[7] = {0, 0, 0, 0, 0, 0, 0};
                     for (int r = 0; r < 32; ++r) {
                         const size_t ri = (size_t)b * 32 + (size_t)r;
@@ -515,13 +531,15 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                                 if ((m[w] >> k) & 1u) lists[r].push_back((uint16_t)(8 * (64 * w + k)));
                         n_iter = std::max(n_iter, lists[r].size());
                     }
-                    put32(body, (uint32_t)n_iter);
+                    n_iter = (n_iter + 1) & ~size_t(1);
+                    sum_iter += (uint32_t)n_iter;
+                    put32(body, (uint32_t)(n_iter / 2));
                     for (int k = 0; k < 7; ++k) put32(body, masks[k]);
-                    for (size_t i = 0; i < n_iter; ++i)
+                    for (size_t i = 0; i < n_iter; i += 2)
                         for (int r = 0; r < 32; ++r) {
-                            const uint16_t o = i < lists[r].size() ? lists[r][i] : zero_off;
-                            body.push_back((uint8_t)(o & 0xFFu));
-                            body.push_back((uint8_t)(o >> 8));
+                            const uint16_t o0 = i < lists[r].size() ? lists[r][i] : zero_off;
+                            const uint16_t o1 = i + 1 < lists[r].size() ? lists[r][i + 1] : zero_off;
+                            put32(body, (uint32_t)o0 | ((uint32_t)o1 << 16));
                         }
                 }
             }
@@ -563,7 +581,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             img.n_narrow_terms += (flags & TF_NARROW) ? 1 : 0;
             img.n_hybrid_terms += (flags & TF_HYBRID) ? 1 : 0;
             img.n_columns += n_np + n_hp + n_pp + n_ph;
-            img.work_ops += term_work(W, flags, n_cls, n_hp, n_pp, n_ph);
+            img.work_ops += term_work(W, flags, n_cls, n_hp, n_pp, n_ph, (int)nb, (int)sum_iter);
         }
         toff.push_back((int64_t)out.size());
         img.work_ops += graph_work(W);

@@ -223,11 +223,14 @@ __device__ __forceinline__ const uint8_t *eval_terms_warp(const uint8_t *p, uint
         } else {
             const uint8_t *blk = p + term_blocks_off(h);
             for (uint32_t b = 0; b < h.nb; ++b) {
-                const uint32_t n_iter = *(const uint32_t *)blk;
-                const uint16_t *ix = (const uint16_t *)(blk + BLOCK_HEAD_BYTES) + lane;
+                const uint32_t n_pairs = *(const uint32_t *)blk;
+                const uint32_t *ix = (const uint32_t *)(blk + BLOCK_HEAD_BYTES) + lane;
                 uint64_t acc = 0;
-#pragma unroll 4
-                for (uint32_t i = 0; i < n_iter; ++i) acc ^= *(const uint64_t *)(sw + ix[32 * i]);
+#pragma unroll 2
+                for (uint32_t i = 0; i < n_pairs; ++i) {
+                    const uint32_t x = ix[32 * i];
+                    acc ^= *(const uint64_t *)(sw + (x & 0xFFFFu)) ^ *(const uint64_t *)(sw + (x >> 16));
+                }
                 if (S > 1) {
                     uint32_t x0 = (uint32_t)acc, x1 = (uint32_t)(acc >> 32);
                     transpose32x2(x0, x1, lane);
@@ -236,7 +239,7 @@ __device__ __forceinline__ const uint8_t *eval_terms_warp(const uint8_t *p, uint
                 } else {
                     wb[b * wstride] = transpose32((uint32_t)acc, lane);
                 }
-                blk += BLOCK_HEAD_BYTES + 64 * n_iter;
+                blk += BLOCK_HEAD_BYTES + 128 * n_pairs;
             }
             RowBits bits[S];
 #pragma unroll

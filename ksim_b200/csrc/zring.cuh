@@ -412,12 +412,15 @@ KS_HD void ph_update(Zr<T> &z, uint32_t pa, uint32_t pb, uint32_t K)
 //   NodePhases class 0, 2, 1, 3 | HalfPi | (a zero row if needed to make the
 //   next position even) | PiProducts (psi, phi) pairs | PhasePairs (alpha,
 //   beta) pairs
-// After the header (and approximation): u16 dead_pw per class-0 row, u8 word
-// (ja | K<<2 | jb<<3 | jg<<5) per PhasePairs column, padded to 16 bytes;
-// then nb blocks of 32 rows, each a 32-byte head
-//   u32 n_iter, u32 masks P1, P2, P4, E3, E1, PP, K0 (bit i = row 32b + i)
-// and n_iter x 32 u16 byte offsets (8 x bit index; entry [i][r] = the i-th
-// set bit of row r of the block, 8 x 64W, the zero word, when it has fewer).
+// After the header (and approximation) the term's constants: the floatfactor
+// times w^(k + phase index) for k = 0..7 (8 x 4 i32, so the final rotation
+// and the floatfactor are one table read and one product), u16 dead_pw per
+// class-0 row, u8 word (ja | K<<2 | jb<<3 | jg<<5) per PhasePairs column,
+// padded to 16 bytes; then nb blocks of 32 rows, each a 32-byte head
+//   u32 n_pairs, u32 masks P1, P2, P4, E3, E1, PP, K0 (bit i = row 32b + i)
+// and n_pairs x 32 u32 words of two u16 byte offsets (8 x bit index; word
+// [i][r] holds the set bits 2i and 2i + 1 of row r of the block, 8 x 64W,
+// the zero word, where it has fewer).
 // Every sum the term needs is linear in the row bits w of a block:
 //   rotation  += popc(w & P1) + 2 popc(w & P2) + 4 popc(w & (P4 | PP & w >> 1))
 //     (P2 and P4 hold the NodePhases classes 1-3, whose sign count enters as
@@ -428,9 +431,20 @@ KS_HD void ph_update(Zr<T> &z, uint32_t pa, uint32_t pb, uint32_t K)
 //   kill: the first row of w & K0 (class 0) with its dead_pw.
 constexpr int BLOCK_HEAD_BYTES = 32;
 KS_HD int term_meta_off(const TermHdr &h) { return TERM_HDR_BYTES + ((h.flags & TF_APX) ? TERM_APX_BYTES : 0); }
+constexpr int TERM_FFK_BYTES = 128;
 KS_HD int term_blocks_off(const TermHdr &h)
 {
-    return term_meta_off(h) + ((2 * (int)h.n_cls[0] + (int)h.n_ph + 15) & ~15);
+    return term_meta_off(h) + TERM_FFK_BYTES + ((2 * (int)h.n_cls[0] + (int)h.n_ph + 15) & ~15);
+}
+KS_HD void load_i32x4(const uint8_t *p, int32_t (&r)[4])
+{
+#if defined(__CUDA_ARCH__)
+    const int4 x = *(const int4 *)p;
+    r[0] = x.x; r[1] = x.y; r[2] = x.z; r[3] = x.w;
+#else
+    const int32_t *q = (const int32_t *)p;
+    r[0] = q[0]; r[1] = q[1]; r[2] = q[2]; r[3] = q[3];
+#endif
 }
 // Position of the first PhasePairs row.
 KS_HD int term_ph_row0(const TermHdr &h)
@@ -473,13 +487,13 @@ KS_HD void term_words_shot(const uint8_t *p, const TermHdr &h, const uint64_t (&
     const uint8_t *blk = p + term_blocks_off(h);
     for (int b = 0; b <= NB_MAX; ++b) out[b] = 0;
     for (uint32_t b = 0; b < h.nb; ++b) {
-        const uint32_t n_iter = *(const uint32_t *)blk;
-        const uint16_t *ix = (const uint16_t *)(blk + BLOCK_HEAD_BYTES);
+        const uint32_t n_pairs = *(const uint32_t *)blk;
+        const uint32_t *ix = (const uint32_t *)(blk + BLOCK_HEAD_BYTES);
         uint32_t word = 0;
         for (int r = 0; r < 32; ++r) {
             uint32_t par = 0;
-            for (uint32_t i = 0; i < n_iter; ++i) {
-                const uint32_t k = (uint32_t)ix[i * 32 + r] >> 3;
+            for (uint32_t i = 0; i < 2 * n_pairs; ++i) {
+                const uint32_t k = ((ix[(i >> 1) * 32 + r] >> (16 * (i & 1u))) & 0xFFFFu) >> 3;
                 uint64_t bit = 0;
 #pragma unroll
                 for (int w = 0; w < W; ++w) bit |= ((uint32_t)w == (k >> 6)) ? (v[w] >> (k & 63u)) & 1u : 0u;
@@ -488,7 +502,7 @@ KS_HD void term_words_shot(const uint8_t *p, const TermHdr &h, const uint64_t (&
             word |= par << r;
         }
         out[b] = word;
-        blk += BLOCK_HEAD_BYTES + 64 * n_iter;
+        blk += BLOCK_HEAD_BYTES + 128 * n_pairs;
     }
 }
 
@@ -504,8 +518,8 @@ template <typename TN, typename T, int S>
 KS_HD const uint8_t *eval_term_rows(const uint8_t *p, const TermHdr &h, const RowBits (&bits)[S], TermOut (&o)[S])
 {
     const uint8_t *meta = p + term_meta_off(h);
-    const uint16_t *dead_pw = (const uint16_t *)meta;
-    const uint8_t *ph_cw = meta + 2 * h.n_cls[0];
+    const uint16_t *dead_pw = (const uint16_t *)(meta + TERM_FFK_BYTES);
+    const uint8_t *ph_cw = meta + TERM_FFK_BYTES + 2 * h.n_cls[0];
     // the block sums: rotation, lambda exponent, class-0 kill
     uint32_t rot[S], lam[S], alive[S];
     int32_t pw[S];  // halvings within one term stay far below 2^31
@@ -533,7 +547,7 @@ KS_HD const uint8_t *eval_term_rows(const uint8_t *p, const TermHdr &h, const Ro
             rot[s] += popc32(w & P1) + 2u * popc32(w & P2) + 4u * popc32(w & (P4 | (PP & (w >> 1))));
             lam[s] += popc32((w & E3) | (~w & E1));
         }
-        blk += BLOCK_HEAD_BYTES + 64 * m[0];
+        blk += BLOCK_HEAD_BYTES + 128 * m[0];
     }
     // NodePhases: C * lambda^(m3 - m1); its rotation w^(6 (m1 + m2 + m3)) is
     // in rot with the HalfPi and PiProducts ones (units: they change no
@@ -593,13 +607,15 @@ KS_HD const uint8_t *eval_term_rows(const uint8_t *p, const TermHdr &h, const Ro
             pw[s] += (int32_t)red;
         }
     }
-    // prefactor: w^(NodePhases + HalfPi + PiProducts + idx), then the exact
-    // floatfactor with one renormalisation
-    const Zr<T> ff = {(T)h.ff.a, (T)h.ff.b, (T)h.ff.c, (T)h.ff.d};
+    // prefactor: w^(NodePhases + HalfPi + PiProducts + idx) times the exact
+    // floatfactor (one product with the tabulated ff * w^k), then one
+    // renormalisation
 #pragma unroll
     for (int s = 0; s < S; ++s) {
-        Zr<T> zz = rot_var(z[s], (rot[s] + h.pf_idx) & 7u);
-        zz = zmul(zz, ff);
+        int32_t f[4];
+        load_i32x4(meta + 16 * (rot[s] & 7u), f);
+        const Zr<T> ffk = {(T)(int64_t)f[0], (T)(int64_t)f[1], (T)(int64_t)f[2], (T)(int64_t)f[3]};
+        Zr<T> zz = zmul(z[s], ffk);
         zreduce(zz, pw[s]);
         if constexpr (sizeof(T) == 8) {
             o[s].z = zz;
