@@ -28,6 +28,7 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <map>
 
 #include "zring.cuh"
 
@@ -266,13 +267,22 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             std::vector<uint8_t> rec;  // column records of this term (exact path)
             struct Row { std::vector<uint64_t> m; uint32_t c; };
             std::vector<Row> hp_rows, pair_rows, ph_rows;  // parity rows (fast paths)
-            double L = 0;              // log2 bound on max_k |sigma_k(z)| (z starts at 1)
-            double Lmax = 0;
+            // Bounds, as log2 of max_k |sigma_k(z)| (>= every coefficient):
+            //   ref_max: every value the reference's step-by-step arithmetic
+            //     holds (its int64 must not wrap, else the term takes the exact
+            //     path, which wraps like it);
+            //   fast_max: every value the fast path must know exactly — after
+            //     each PhasePairs factor (the evenness test and halving) and
+            //     at the end; everything between is ring arithmetic that may
+            //     wrap.  The NodePhases result itself must be exact only
+            //     where it is widened (the hybrid path).
+            double L = 0;  // z starts at 1
+            double ref_max = 0, fast_max = 0;
             const double kLim = 62.0 - 1e-9;
             bool unsafe = false;
-            auto step = [&](double transient) {
-                Lmax = std::max(Lmax, transient);
-                if (transient > kLim) unsafe = true;
+            auto step = [&](double v) {
+                ref_max = std::max(ref_max, v);
+                fast_max = std::max(fast_max, v);
             };
             // NodePhases.  A column's mask carries the constant bit iff bit 2
             // of its phase is set, so its parity is the sign of w^(4 par):
@@ -326,12 +336,9 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             bool c_ok = true;
             for (int r = 0; r < cnp; ++r) {
                 const uint32_t j = npc[order[r]].phase & 3u;
-                if (j == 0) {
-                    step(L + 1.0);  // 2z before it is halved back
-                } else {
+                if (j != 0) {
                     nu += (j & 1u) ? 1u : 2u;
                     L += (j & 1u) ? std::log2(2.0 * std::cos(M_PI / 8)) : 0.5;
-                    step(L);
                     // C *= 1 + w^j: w = (0,1,0,0), i = (0,0,1,0), w^3 = (0,0,0,-1)
                     const __int128 a = C[0], b = C[1], c = C[2], d = C[3];
                     if (j == 1) { C[0] = a + d; C[1] = b + a; C[2] = c + b; C[3] = d - c; }
@@ -352,7 +359,20 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             }
             const int n_np = cnp;
             const int32_t np_halvings = n_cls[0] + (int32_t)std::count(np_red.begin(), np_red.end(), 1u);
-            const double Lmax_np = Lmax;  // the NodePhases block's bound
+            // The reference runs the block in its own order.  Each factor adds
+            // log|f| >= nu / 4 to the bound (odd j: 0.89 >= 0.25; j = 2: 0.5;
+            // j = 0: 1), so in any order a value after a factor is below
+            // 2^(S + 0.75) with S = sum (log|f| - nu / 4) over all the block's
+            // factors, and the factor-2 transient (2z before its halving)
+            // below 2^(S + 1.75).
+            const double L_np = L;  // the block's result
+            if (cnp > 0) ref_max = std::max(ref_max, L_np - (double)nu / 4.0 + 1.75);
+            ref_max = std::max(ref_max, L_np);
+            // PhasePairs: the bound per valuation of z ((1 - w)-adic; the
+            // block's result has nu = the leftover above, for every shot
+            // whose term survives)
+            std::map<uint32_t, double> ph_state;
+            ph_state[nu] = L_np;
             // HalfPi
             int n_hp = 0;
             for (int c = 0; c < g.Thp; ++c) {
@@ -410,15 +430,29 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 if (b2) mask[2 * W - 1] |= one_bit;
                 const uint32_t K = ((gc >> 2) ^ 1u ^ a2 ^ b2) & 1u;
                 uint64_t cw = (ac & 3u) | (K << 2) | ((bc & 3u) << 3) | ((gc & 3u) << 5);
-                double fmax = 0;
+                // bound through the factor for each valuation state: the value
+                // after it is an exact point; the reference then halves once
+                // iff nu >= 4 (a zero factor ends the term)
+                std::map<uint32_t, double> next;
                 for (uint32_t combo = 0; combo < 4; ++combo) {  // combo = raw pa | pb << 1
                     int64_t f[4];
                     phase_pair((int)(ac ^ ((combo & 1u) << 2)), (int)(bc ^ ((combo >> 1) << 2)), f);
-                    fmax = std::max(fmax, max_embed(f));
+                    const uint32_t v = zw_valuation(f);
+                    if (v == NU_ZERO) continue;
+                    const double lf = std::log2(max_embed(f)) + 1e-12;
+                    for (const auto &sv : ph_state) {
+                        double x = sv.second + lf;
+                        step(x);
+                        uint32_t s1 = sv.first + v;
+                        if (s1 >= 4) {
+                            s1 -= 4;
+                            x -= 1.0;
+                        }
+                        auto it = next.find(s1);
+                        if (it == next.end() || it->second < x) next[s1] = x;
+                    }
                 }
-                step(L + 2.0);  // partial sums of four rotated copies
-                L += fmax > 0 ? std::log2(fmax) + 1e-12 : 0.0;
-                step(L);
+                ph_state.swap(next);
                 ph_rows.push_back({std::vector<uint64_t>(mask.begin(), mask.begin() + W), (uint32_t)cw});
                 ph_rows.push_back({std::vector<uint64_t>(mask.begin() + W, mask.begin() + 2 * W), 0});
                 for (int w = 0; w < 2 * W; ++w) put64(rec, mask[w]);
@@ -431,14 +465,15 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             const int64_t ff64[4] = {ff[0], ff[1], ff[2], ff[3]};
             const double S = std::fabs((double)ff[0]) + std::fabs((double)ff[1]) +
                              std::fabs((double)ff[2]) + std::fabs((double)ff[3]);
-            if (S > 0) step(L + std::log2(S) + 1e-12);
+            if (S > 0)
+                for (const auto &sv : ph_state) step(sv.second + std::log2(S) + 1e-12);
             if (n_np > 0xFFFF || n_hp > 0xFFFF || n_pp > 0xFFFF || n_ph > 0xFFFF) {
                 err = gname + ": a term has more than 65535 columns in one family";
                 return KSIM_ERR_UNSUPPORTED;
             }
-            // every value the fast path must know exactly is below 2^Lmax; with
-            // Lmax <= 30.5 it fits int32 and the term runs on 32-bit words
-            // (a fast term's odd classes are far below LAM_MAX columns: each
+            // every value the fast path must know exactly is below
+            // 2^fast_max; with fast_max <= 30.5 it fits int32 and the term
+            // runs on 32-bit words (a fast term's odd classes are far below LAM_MAX columns: each
             // adds about 0.64 to the bound; the check keeps the table lookup
             // in range whatever the bound)
             uint32_t max_dead = 0;
@@ -447,8 +482,9 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             // 32-bit negative)
             bool ff_min = false;
             for (int i = 0; i < 4; ++i) ff_min |= ff[i] == INT32_MIN;
-            if (std::max(n_cls[1], n_cls[3]) > LAM_MAX || !c_ok || max_dead > 0xFFFFu || ff_min) unsafe = true;
-            uint32_t flags = unsafe ? TF_SLOW : (Lmax <= 30.5 ? TF_NARROW : (Lmax_np <= 30.5 ? TF_HYBRID : 0u));
+            if (ref_max > kLim || std::max(n_cls[1], n_cls[3]) > LAM_MAX || !c_ok || max_dead > 0xFFFFu || ff_min)
+                unsafe = true;
+            uint32_t flags = unsafe ? TF_SLOW : (fast_max <= 30.5 ? TF_NARROW : (L_np <= 30.5 ? TF_HYBRID : 0u));
             // the fast paths' parity rows (row order and block masks:
             // zring.cuh); more than NB_MAX blocks of them sends the term to
             // the exact path
