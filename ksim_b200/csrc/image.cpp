@@ -119,12 +119,15 @@ bool all_zero(const uint64_t *m, int W)
 //     transposes: 2 x 5 rounds x 2 (rotate, select) x 32 lanes / 64 = 10
 //     block sums: 4 (and) + 4 (popcount) + 1 (shift) + 4 (accumulate) = 13
 //   NodePhases: C * lambda^e, 16 multiply-adds x c_np + 4 (mask) + 2
-//   PhasePairs: 3 (bits) + 3 (signs) + 12c (three rotated adds)
+//   PhasePairs with a rotation 0: 3 (bits) + 2 (sign) + 4c (signed copy)
+//               + 4c (select) + 4 (zero test, pw)
+//   other PhasePairs: 3 (bits) + 3 (signs) + 12c (three rotated adds)
 //               + 4 (evenness) + 4c + 1 (conditional halving)
 //   per term: ff * w^k read 4, floatfactor product 16 (c = 1) or 64 (c = 2),
 //             renormalisation 6c, complex value and sum 16
 //   per graph: parameter vector 4W + 8, ballot words 4, Bernoulli step 10
-double term_work(int W, uint32_t flags, const int n_cls[4], int n_hp, int n_pp, int n_ph, int nb, int sum_iter)
+double term_work(int W, uint32_t flags, const int n_cls[4], int n_hp, int n_pp, int n_ph, int n_ph_unit, int nb,
+                 int sum_iter)
 {
     const double par = 3.0 * W + 2.0;
     const int n_np = n_cls[0] + n_cls[1] + n_cls[2] + n_cls[3];
@@ -135,7 +138,8 @@ double term_work(int W, uint32_t flags, const int n_cls[4], int n_hp, int n_pp, 
     double w = (double)sum_iter + 23.0 * nb;
     if (n_cls[1] | n_cls[3]) w += 16.0 * cn + 2.0;
     w += 4.0 * cn;
-    w += n_ph * (3.0 + 3.0 + 12.0 * c + 4.0 + 4.0 * c + 1.0);
+    w += n_ph_unit * (3.0 + 2.0 + 8.0 * c + 4.0);
+    w += (n_ph - n_ph_unit) * (3.0 + 3.0 + 12.0 * c + 4.0 + 4.0 * c + 1.0);
     w += 4.0 + (c == 1.0 ? 16.0 : 64.0) + 6.0 * c + 16.0;
     return w;
 }
@@ -413,7 +417,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 ++n_pp;
             }
             // PhasePairs
-            int n_ph = 0;
+            int n_ph = 0, n_ph_unit = 0;
             for (int c = 0; c < cph; ++c) {
                 const size_t ci = (size_t)t * g.Tph + c;
                 if (!pack_mask(g.ph_alpha_p + ci * P, P, W, mask.data()) ||
@@ -422,6 +426,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                     return KSIM_ERR_MALFORMED_PROGRAM;
                 }
                 const uint32_t ac = g.ph_alpha[ci] & 7u, bc = g.ph_beta[ci] & 7u, gc = (ac + bc) & 7u;
+                if ((ac & 3u) == 0 || (bc & 3u) == 0) ++n_ph_unit;
                 const uint32_t a2 = ac >> 2, b2 = bc >> 2;
                 // the masks carry bit 2 of alpha / beta in the constant bit, so
                 // pa' = pa ^ a2 and pb' = pb ^ b2 are the signs of the w^a and
@@ -617,7 +622,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             img.n_narrow_terms += (flags & TF_NARROW) ? 1 : 0;
             img.n_hybrid_terms += (flags & TF_HYBRID) ? 1 : 0;
             img.n_columns += n_np + n_hp + n_pp + n_ph;
-            img.work_ops += term_work(W, flags, n_cls, n_hp, n_pp, n_ph, (int)nb, (int)sum_iter);
+            img.work_ops += term_work(W, flags, n_cls, n_hp, n_pp, n_ph, n_ph_unit, (int)nb, (int)sum_iter);
         }
         toff.push_back((int64_t)out.size());
         img.work_ops += graph_work(W);

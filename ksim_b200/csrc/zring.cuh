@@ -406,6 +406,41 @@ KS_HD void ph_update(Zr<T> &z, uint32_t pa, uint32_t pb, uint32_t K)
     }
 }
 
+// The reference's renormalisation after a PhasePairs factor: halve once if
+// all four coefficients are even and not all zero (zx_eval.hpp:35-41).
+template <typename T>
+KS_HD void ph_halve(Zr<T> &z, int32_t &pw)
+{
+    const T ov = z.a | z.b | z.c | z.d;
+    const uint32_t red = (ov != 0 && (ov & 1u) == 0) ? 1u : 0u;
+    shr_all(z, red);
+    pw += (int32_t)red;
+}
+
+// A PhasePairs factor one of whose rotations is 0: with a = (-1)^psel (that
+// copy) and b = (-1)^psign w^J (the other), 1 + a + b - ab is 2 (psel = 0) or
+// 2b (psel = 1).  The product is even, so the reference halves it once
+// unless z is zero: z becomes z or (-1)^psign R_J(z), and pw grows by one.
+template <typename T, int J>
+KS_HD void ph_unit(Zr<T> &z, uint32_t psel, uint32_t psign, int32_t &pw)
+{
+    const T ov = z.a | z.b | z.c | z.d;
+    pw += ov != 0 ? 1 : 0;
+    const Sign<T> g = sign_of(psign, T());
+    const T p = g.pos, n = g.neg;
+    Zr<T> r;
+    if constexpr (J == 0) {
+        r.a = sadd((T)0, z.a, p); r.b = sadd((T)0, z.b, p); r.c = sadd((T)0, z.c, p); r.d = sadd((T)0, z.d, p);
+    } else if constexpr (J == 1) {
+        r.a = sadd((T)0, z.d, p); r.b = sadd((T)0, z.a, p); r.c = sadd((T)0, z.b, p); r.d = sadd((T)0, z.c, n);
+    } else if constexpr (J == 2) {
+        r.a = sadd((T)0, z.c, n); r.b = sadd((T)0, z.d, p); r.c = sadd((T)0, z.a, p); r.d = sadd((T)0, z.b, n);
+    } else {
+        r.a = sadd((T)0, z.b, n); r.b = sadd((T)0, z.c, n); r.c = sadd((T)0, z.d, p); r.d = sadd((T)0, z.a, n);
+    }
+    if (psel) z = r;
+}
+
 // ---- fast terms: parity rows -------------------------------------------------
 // A fast term's columns are parity rows over the parameter vector, each
 // stored as the list of its set bits.  Row order (term-relative position):
@@ -587,24 +622,33 @@ KS_HD const uint8_t *eval_term_rows(const uint8_t *p, const TermHdr &h, const Ro
             pa[s] = x & 1u;
             pb[s] = (x >> 1) & 1u;
         }
-        // one branch on the rotation pair; the third rotation is their sum
+        // one branch on the rotation pair; the third rotation is their sum.
+        // A pair with a rotation 0 is a select (ph_unit); the others take the
+        // three rotated adds and the reference's evenness test.
         switch ((cw & 3u) | ((cw >> 1) & 12u)) {
-#define KSIM_PH_CASE(JA, JB)                                                        \
-    case (JA) | ((JB) << 2):                                                        \
-        _Pragma("unroll") for (int s = 0; s < S; ++s) ph_update<T, JA, JB>(z[s], pa[s], pb[s], K); \
+#define KSIM_PH_UNIT_A(JB)                                                             \
+    case (JB) << 2:                                                                    \
+        _Pragma("unroll") for (int s = 0; s < S; ++s) ph_unit<T, JB>(z[s], pa[s], pb[s], pw[s]); \
         break;
-        KSIM_PH_CASE(0, 0) KSIM_PH_CASE(1, 0) KSIM_PH_CASE(2, 0) KSIM_PH_CASE(3, 0)
-        KSIM_PH_CASE(0, 1) KSIM_PH_CASE(1, 1) KSIM_PH_CASE(2, 1) KSIM_PH_CASE(3, 1)
-        KSIM_PH_CASE(0, 2) KSIM_PH_CASE(1, 2) KSIM_PH_CASE(2, 2) KSIM_PH_CASE(3, 2)
-        KSIM_PH_CASE(0, 3) KSIM_PH_CASE(1, 3) KSIM_PH_CASE(2, 3) KSIM_PH_CASE(3, 3)
+#define KSIM_PH_UNIT_B(JA)                                                             \
+    case (JA):                                                                         \
+        _Pragma("unroll") for (int s = 0; s < S; ++s) ph_unit<T, JA>(z[s], pb[s], pa[s], pw[s]); \
+        break;
+#define KSIM_PH_CASE(JA, JB)                                                           \
+    case (JA) | ((JB) << 2):                                                           \
+        _Pragma("unroll") for (int s = 0; s < S; ++s) {                                \
+            ph_update<T, JA, JB>(z[s], pa[s], pb[s], K);                               \
+            ph_halve(z[s], pw[s]);                                                     \
+        }                                                                              \
+        break;
+        KSIM_PH_UNIT_A(0) KSIM_PH_UNIT_A(1) KSIM_PH_UNIT_A(2) KSIM_PH_UNIT_A(3)
+        KSIM_PH_UNIT_B(1) KSIM_PH_UNIT_B(2) KSIM_PH_UNIT_B(3)
+        KSIM_PH_CASE(1, 1) KSIM_PH_CASE(2, 1) KSIM_PH_CASE(3, 1)
+        KSIM_PH_CASE(1, 2) KSIM_PH_CASE(2, 2) KSIM_PH_CASE(3, 2)
+        KSIM_PH_CASE(1, 3) KSIM_PH_CASE(2, 3) KSIM_PH_CASE(3, 3)
 #undef KSIM_PH_CASE
-        }
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            const T ov = z[s].a | z[s].b | z[s].c | z[s].d;
-            const uint32_t red = (ov != 0 && (ov & 1u) == 0) ? 1u : 0u;
-            shr_all(z[s], red);
-            pw[s] += (int32_t)red;
+#undef KSIM_PH_UNIT_B
+#undef KSIM_PH_UNIT_A
         }
     }
     // prefactor: w^(NodePhases + HalfPi + PiProducts + idx) times the exact
