@@ -221,9 +221,14 @@ __device__ __forceinline__ const uint8_t *eval_terms_warp(const uint8_t *p, uint
 #pragma unroll
             for (int s = 0; s < S; ++s) eval_term_exact_call<W>(p, h, v[s], o[s]);
         } else {
+            RowSums sums[S];
+#pragma unroll
+            for (int s = 0; s < S; ++s) row_sums_init(sums[s], h);
+            const uint16_t *dead_pw = term_dead_pw(p, h);
             const uint8_t *blk = p + term_blocks_off(h);
             for (uint32_t b = 0; b < h.nb; ++b) {
-                const uint32_t n_pairs = *(const uint32_t *)blk;
+                const BlockHead m = load_block_head(blk);
+                const uint32_t n_pairs = m.n_pairs;
                 const uint32_t *ix = (const uint32_t *)(blk + BLOCK_HEAD_BYTES) + lane;
                 uint64_t acc = 0;
 #pragma unroll 2
@@ -236,8 +241,12 @@ __device__ __forceinline__ const uint8_t *eval_terms_warp(const uint8_t *p, uint
                     transpose32x2(x0, x1, lane);
                     wb[b * wstride] = x0;
                     wb[b * wstride + nt] = x1;
+                    row_sums_add(sums[0], x0, m, b, dead_pw);
+                    row_sums_add(sums[S - 1], x1, m, b, dead_pw);
                 } else {
-                    wb[b * wstride] = transpose32((uint32_t)acc, lane);
+                    const uint32_t x0 = transpose32((uint32_t)acc, lane);
+                    wb[b * wstride] = x0;
+                    row_sums_add(sums[0], x0, m, b, dead_pw);
                 }
                 blk += BLOCK_HEAD_BYTES + 128 * n_pairs;
             }
@@ -247,7 +256,7 @@ __device__ __forceinline__ const uint8_t *eval_terms_warp(const uint8_t *p, uint
                 bits[s].w = wb + s * nt;
                 bits[s].stride = wstride;
             }
-            eval_term_rows_any<S>(p, h, bits, o);
+            eval_term_rows_any<S>(p, h, sums, bits, o);
         }
 #pragma unroll
         for (int s = 0; s < S; ++s) {

@@ -549,40 +549,72 @@ KS_HD void term_words_shot(const uint8_t *p, const TermHdr &h, const uint64_t (&
 // parity-row bits.
 // TN: word of the NodePhases block, T: word of the rest (TN = uint32_t, T =
 // uint64_t is the hybrid path: NodePhases proven below 2^31, the rest not).
+// The head of a parity block: index-pair count and the seven role masks.
+struct BlockHead {
+    uint32_t n_pairs, P1, P2, P4, E3, E1, PP, K0;
+};
+KS_HD BlockHead load_block_head(const uint8_t *blk)
+{
+    BlockHead m;
+#if defined(__CUDA_ARCH__)
+    const uint4 x = *(const uint4 *)blk, y = *(const uint4 *)(blk + 16);
+    m.n_pairs = x.x; m.P1 = x.y; m.P2 = x.z; m.P4 = x.w;
+    m.E3 = y.x; m.E1 = y.y; m.PP = y.z; m.K0 = y.w;
+#else
+    const uint32_t *u = (const uint32_t *)blk;
+    m.n_pairs = u[0]; m.P1 = u[1]; m.P2 = u[2]; m.P4 = u[3];
+    m.E3 = u[4]; m.E1 = u[5]; m.PP = u[6]; m.K0 = u[7];
+#endif
+    return m;
+}
+
+// A shot's running sums over a fast term's blocks: rotation (mod 8), lambda
+// exponent (+ n1), and the class-0 kill with its pw.
+struct RowSums {
+    uint32_t rot, lam, alive;
+    int32_t pw;  // halvings within one term stay far below 2^31
+};
+KS_HD void row_sums_init(RowSums &a, const TermHdr &h)
+{
+    a.rot = 0;
+    a.lam = 0;
+    a.alive = 1;
+    a.pw = h.np_pw;
+}
+// Block b with row-parity word w.
+KS_HD void row_sums_add(RowSums &a, uint32_t w, const BlockHead &m, uint32_t b, const uint16_t *dead_pw)
+{
+    if (m.K0) {
+        const uint32_t k = w & m.K0;
+        if (k != 0 && a.alive) {
+            a.pw = (int32_t)dead_pw[32 * b + (uint32_t)ffs32(k)];
+            a.alive = 0;
+        }
+    }
+    a.rot += popc32(w & m.P1) + 2u * popc32(w & m.P2) + 4u * popc32(w & (m.P4 | (m.PP & (w >> 1))));
+    a.lam += popc32((w & m.E3) | (~w & m.E1));
+}
+KS_HD const uint16_t *term_dead_pw(const uint8_t *p, const TermHdr &h)
+{
+    return (const uint16_t *)(p + term_meta_off(h) + TERM_FFK_BYTES);
+}
+
+// The rest of a fast term from its block sums (a) and its row-parity bits
+// (read for the PhasePairs rows).
 template <typename TN, typename T, int S>
-KS_HD const uint8_t *eval_term_rows(const uint8_t *p, const TermHdr &h, const RowBits (&bits)[S], TermOut (&o)[S])
+KS_HD const uint8_t *eval_term_rows(const uint8_t *p, const TermHdr &h, const RowSums (&sums)[S],
+                                    const RowBits (&bits)[S], TermOut (&o)[S])
 {
     const uint8_t *meta = p + term_meta_off(h);
-    const uint16_t *dead_pw = (const uint16_t *)(meta + TERM_FFK_BYTES);
     const uint8_t *ph_cw = meta + TERM_FFK_BYTES + 2 * h.n_cls[0];
-    // the block sums: rotation, lambda exponent, class-0 kill
     uint32_t rot[S], lam[S], alive[S];
-    int32_t pw[S];  // halvings within one term stay far below 2^31
+    int32_t pw[S];
 #pragma unroll
     for (int s = 0; s < S; ++s) {
-        rot[s] = 0;
-        lam[s] = 0;
-        alive[s] = 1;
-        pw[s] = h.np_pw;
-    }
-    const uint8_t *blk = p + term_blocks_off(h);
-    for (uint32_t b = 0; b < h.nb; ++b) {
-        const uint32_t *m = (const uint32_t *)blk;
-        const uint32_t P1 = m[1], P2 = m[2], P4 = m[3], E3 = m[4], E1 = m[5], PP = m[6], K0 = m[7];
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            const uint32_t w = bits[s].word((int)b);
-            if (K0) {
-                const uint32_t k = w & K0;
-                if (k != 0 && alive[s]) {
-                    pw[s] = (int32_t)dead_pw[32 * b + (uint32_t)ffs32(k)];
-                    alive[s] = 0;
-                }
-            }
-            rot[s] += popc32(w & P1) + 2u * popc32(w & P2) + 4u * popc32(w & (P4 | (PP & (w >> 1))));
-            lam[s] += popc32((w & E3) | (~w & E1));
-        }
-        blk += BLOCK_HEAD_BYTES + 128 * m[0];
+        rot[s] = sums[s].rot;
+        lam[s] = sums[s].lam;
+        alive[s] = sums[s].alive;
+        pw[s] = sums[s].pw;
     }
     // NodePhases: C * lambda^(m3 - m1); its rotation w^(6 (m1 + m2 + m3)) is
     // in rot with the HalfPi and PiProducts ones (units: they change no
@@ -675,12 +707,12 @@ KS_HD const uint8_t *eval_term_rows(const uint8_t *p, const TermHdr &h, const Ro
 
 // A fast term on the path its header selects.
 template <int S>
-KS_HD const uint8_t *eval_term_rows_any(const uint8_t *p, const TermHdr &h, const RowBits (&bits)[S],
-                                        TermOut (&o)[S])
+KS_HD const uint8_t *eval_term_rows_any(const uint8_t *p, const TermHdr &h, const RowSums (&sums)[S],
+                                        const RowBits (&bits)[S], TermOut (&o)[S])
 {
-    if (h.flags & TF_NARROW) return eval_term_rows<uint32_t, uint32_t, S>(p, h, bits, o);
-    if (h.flags & TF_HYBRID) return eval_term_rows<uint32_t, uint64_t, S>(p, h, bits, o);
-    return eval_term_rows<uint64_t, uint64_t, S>(p, h, bits, o);
+    if (h.flags & TF_NARROW) return eval_term_rows<uint32_t, uint32_t, S>(p, h, sums, bits, o);
+    if (h.flags & TF_HYBRID) return eval_term_rows<uint32_t, uint64_t, S>(p, h, sums, bits, o);
+    return eval_term_rows<uint64_t, uint64_t, S>(p, h, sums, bits, o);
 }
 
 // Exact path: the reference's step-by-step arithmetic (zx_eval.hpp:101-165),
@@ -778,13 +810,22 @@ KS_HD const uint8_t *eval_term_s(const uint8_t *p, const TermHdr &h, const uint6
     }
     uint32_t words[S][NB_MAX + 1];
     RowBits bits[S];
+    RowSums sums[S];
+    const uint16_t *dead_pw = term_dead_pw(p, h);
 #pragma unroll
     for (int s = 0; s < S; ++s) {
         term_words_shot<W>(p, h, v[s], words[s]);
         bits[s].w = words[s];
         bits[s].stride = 1;
+        row_sums_init(sums[s], h);
+        const uint8_t *blk = p + term_blocks_off(h);
+        for (uint32_t b = 0; b < h.nb; ++b) {
+            const BlockHead m = load_block_head(blk);
+            row_sums_add(sums[s], words[s][b], m, b, dead_pw);
+            blk += BLOCK_HEAD_BYTES + 128 * m.n_pairs;
+        }
     }
-    return eval_term_rows_any<S>(p, h, bits, o);
+    return eval_term_rows_any<S>(p, h, sums, bits, o);
 }
 
 // One term for one shot.
