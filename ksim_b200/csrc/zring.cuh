@@ -272,21 +272,32 @@ KS_HD void set_one_bit(uint64_t (&v)[W])
 
 KS_HD TermHdr load_hdr(const uint8_t *p)
 {
-    const uint32_t *u = (const uint32_t *)p;
-    const uint32_t w0 = u[0], w1 = u[1], w2 = u[2];
+    uint32_t u[12], nb;
+#if defined(__CUDA_ARCH__)
+    const uint4 *q = (const uint4 *)p;  // records are 16-byte aligned
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const uint4 x = q[i];
+        u[4 * i] = x.x; u[4 * i + 1] = x.y; u[4 * i + 2] = x.z; u[4 * i + 3] = x.w;
+    }
+    nb = q[5].x;
+#else
+    const uint32_t *q = (const uint32_t *)p;
+    for (int i = 0; i < 12; ++i) u[i] = q[i];
+    nb = q[20];
+#endif
     TermHdr h;
-    h.n_np = w0 & 0xFFFFu; h.n_hp = w0 >> 16;
-    h.n_pp = w1 & 0xFFFFu; h.n_ph = w1 >> 16;
-    h.pf_idx = w2 & 7u; h.flags = (w2 >> 16) & 0xFFu;
+    h.n_np = u[0] & 0xFFFFu; h.n_hp = u[0] >> 16;
+    h.n_pp = u[1] & 0xFFFFu; h.n_ph = u[1] >> 16;
+    h.pf_idx = u[2] & 7u; h.flags = (u[2] >> 16) & 0xFFu;
     h.power2 = (int32_t)u[3];
-    const int32_t *ff = (const int32_t *)(p + 16);
-    h.ff.a = (uint64_t)(int64_t)ff[0]; h.ff.b = (uint64_t)(int64_t)ff[1];
-    h.ff.c = (uint64_t)(int64_t)ff[2]; h.ff.d = (uint64_t)(int64_t)ff[3];
+    h.ff.a = (uint64_t)(int64_t)(int32_t)u[4]; h.ff.b = (uint64_t)(int64_t)(int32_t)u[5];
+    h.ff.c = (uint64_t)(int64_t)(int32_t)u[6]; h.ff.d = (uint64_t)(int64_t)(int32_t)u[7];
     h.n_cls[0] = u[8] & 0xFFFFu; h.n_cls[1] = u[8] >> 16;
     h.n_cls[2] = u[9] & 0xFFFFu; h.n_cls[3] = u[9] >> 16;
     h.np_pw = (int32_t)u[10];
     h.rec_bytes = u[11];
-    h.nb = u[20];
+    h.nb = nb;
     return h;
 }
 
