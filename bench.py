@@ -56,7 +56,7 @@ L2_FLUSH_BYTES = 256 << 20
 # k_sample on the same workload at 262,144 shots (dram__bytes_read.sum +
 # dram__bytes_write.sum), plus the output row the capture's L2 absorbed;
 # scaled to a launch by its shots.  Source: profiles/k_sample_cfg2_current.md.
-NCU_DRAM_BYTES_PER_SHOT = {"cfg2-medium-40q-t12": 67.0 + 40.0}
+NCU_DRAM_BYTES_PER_SHOT = {"cfg2-medium-40q-t12": 66.2 + 40.0}
 
 
 def parse():
