@@ -148,15 +148,32 @@ __device__ __forceinline__ uint32_t get_bit(const uint64_t (&v)[W], int pos)
     return x != 0 ? 1u : 0u;
 }
 
-// 32x32 bit transposes across the warp, two at once: lane i holds row i of
-// each (bit b = column b) and gets column i back (bit b = row b).  Round j
-// swaps the off-diagonal j x j blocks of lane pairs (i, i ^ j).
+// 32x32 bit transposes across the warp: lane i holds row i (bit b = column
+// b) and gets column i back (bit b = row b).  Round j swaps the off-diagonal
+// j x j blocks of lane pairs (i, i ^ j): the lower lane keeps its bits with
+// b & j clear and takes its partner's, shifted up by j, into the others; the
+// upper lane the mirror image.  The 16- and 8-bit rounds move whole bytes,
+// one byte permute each; the 4-, 2- and 1-bit rounds rotate and merge.
+__device__ __forceinline__ uint32_t tr_round_bytes(uint32_t x, uint32_t y, int j, bool up)
+{
+    // lower: [x0 x1 y0 y1] (j = 16) or [x0 y0 x2 y2] (j = 8); upper the mirror
+    const uint32_t sel = j == 16 ? (up ? 0x3276u : 0x5410u) : (up ? 0x3715u : 0x6240u);
+    return __byte_perm(x, y, sel);
+}
+
 __device__ __forceinline__ void transpose32x2(uint32_t &x0, uint32_t &x1, int lane)
 {
 #pragma unroll
-    for (int j = 16; j >= 1; j >>= 1) {
-        const uint32_t m = j == 16 ? 0xFFFF0000u : j == 8 ? 0xFF00FF00u : j == 4 ? 0xF0F0F0F0u
-                         : j == 2 ? 0xCCCCCCCCu : 0xAAAAAAAAu;  // bits b with b & j
+    for (int j = 16; j >= 8; j >>= 1) {
+        const bool up = (lane & j) != 0;
+        const uint32_t y0 = __shfl_xor_sync(~0u, x0, j);
+        const uint32_t y1 = __shfl_xor_sync(~0u, x1, j);
+        x0 = tr_round_bytes(x0, y0, j, up);
+        x1 = tr_round_bytes(x1, y1, j, up);
+    }
+#pragma unroll
+    for (int j = 4; j >= 1; j >>= 1) {
+        const uint32_t m = j == 4 ? 0xF0F0F0F0u : j == 2 ? 0xCCCCCCCCu : 0xAAAAAAAAu;  // bits b with b & j
         const bool up = (lane & j) != 0;
         const uint32_t keep = up ? m : ~m;
         const uint32_t sh = up ? (uint32_t)j : (uint32_t)(32 - j);  // rotate right by j, or left by j
@@ -170,9 +187,13 @@ __device__ __forceinline__ void transpose32x2(uint32_t &x0, uint32_t &x1, int la
 __device__ __forceinline__ uint32_t transpose32(uint32_t x0, int lane)
 {
 #pragma unroll
-    for (int j = 16; j >= 1; j >>= 1) {
-        const uint32_t m = j == 16 ? 0xFFFF0000u : j == 8 ? 0xFF00FF00u : j == 4 ? 0xF0F0F0F0u
-                         : j == 2 ? 0xCCCCCCCCu : 0xAAAAAAAAu;
+    for (int j = 16; j >= 8; j >>= 1) {
+        const uint32_t y0 = __shfl_xor_sync(~0u, x0, j);
+        x0 = tr_round_bytes(x0, y0, j, (lane & j) != 0);
+    }
+#pragma unroll
+    for (int j = 4; j >= 1; j >>= 1) {
+        const uint32_t m = j == 4 ? 0xF0F0F0F0u : j == 2 ? 0xCCCCCCCCu : 0xAAAAAAAAu;
         const bool up = (lane & j) != 0;
         const uint32_t keep = up ? m : ~m;
         const uint32_t sh = up ? (uint32_t)j : (uint32_t)(32 - j);
