@@ -275,7 +275,7 @@ typedef struct ksim_batch_job {
 } ksim_batch_job;
 
 /* Launch shape of a batch (zero / negative fields take the defaults:
- * 256 threads, 16 KiB slots, CTAs per SM from occupancy, graph on). */
+ * 128 threads, 16 KiB slots, CTAs per SM from occupancy, graph on). */
 typedef struct ksim_batch_tuning {
     int32_t threads;      /* shots per work item (one per thread), multiple of 32, <= 256 */
     int32_t slot_bytes;   /* staging slot, multiple of 16, >= every job's largest term */

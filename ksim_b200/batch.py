@@ -31,7 +31,7 @@ from .sampler import B200ProgramSampler
 
 __all__ = ["BatchSampler", "tune_cache_path"]
 
-_DEFAULT_TUNING = {"threads": 256, "slot_bytes": 16384, "ctas_per_sm": 0}
+_DEFAULT_TUNING = {"threads": 128, "slot_bytes": 16384, "ctas_per_sm": 0}
 _CANDIDATES = [
     {"threads": t, "slot_bytes": s, "ctas_per_sm": c}
     for t in (128, 256) for s in (8192, 16384, 32768) for c in (0, 2)
@@ -118,7 +118,7 @@ class BatchSampler:
         jobs = self._jobs()
         self._n_jobs = len(jobs)
         arr = (_abi.BatchJob * max(len(jobs), 1))(*jobs)
-        t = _abi.BatchTuning(int(tuning.get("threads", 256)), int(tuning.get("slot_bytes", 16384)),
+        t = _abi.BatchTuning(int(tuning.get("threads", 128)), int(tuning.get("slot_bytes", 16384)),
                              int(tuning.get("ctas_per_sm", 0)), 1 if self.use_graph else 0)
         h = ctypes.c_void_p()
         check(self.L.ksim_batch_create(arr, len(jobs), ctypes.byref(t), ctypes.byref(h)))

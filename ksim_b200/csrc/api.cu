@@ -172,7 +172,7 @@ ksim_status ksim_component_create(const ksim_graph_desc *graphs, int32_t n_graph
     // default launch shape: slot fits the largest term and at least 16 KiB;
     // staging is skipped when two slots would not fit in shared memory
     const int64_t slot = std::max<int64_t>(16384, (c->img.max_term_bytes + 15) & ~int64_t(15));
-    c->cfg.threads = 256;
+    c->cfg.threads = 128;  // 4 CTAs of 128 per SM: a quarter of the warps per barrier
     c->cfg.slot_bytes = (int)std::min<int64_t>(slot, 1 << 30);
     c->cfg.staged =
         sample_smem_bytes((int)std::min<int64_t>(slot, 1 << 20), true, c->img.W, c->cfg.threads) <= 200 * 1024 ? 1

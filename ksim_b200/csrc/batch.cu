@@ -95,7 +95,7 @@ using namespace ksim;
 
 struct ksim_batch {
     int device = 0;
-    int threads = 256, slot_bytes = 16384, ctas_per_sm = 0, use_graph = 1;
+    int threads = 128, slot_bytes = 16384, ctas_per_sm = 0, use_graph = 1;
     std::vector<ksim_component *> comps;
     std::vector<BatchJobDev> host_jobs;
     BatchJobDev *d_jobs = nullptr;
