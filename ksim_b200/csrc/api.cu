@@ -622,8 +622,8 @@ ksim_status program_sample_host(ksim_program *p, const uint8_t *f, int64_t B, in
     uint8_t *d_in = packed ? (uint8_t *)p->ws_fp.p : d_f;       // where the host rows land
     uint8_t *d_back = packed ? (uint8_t *)p->ws_op.p : d_out;   // what goes back
 
-    // chunks: about a quarter of the shots each, at least 128 Ki shots
-    const int64_t chunk = std::max<int64_t>((int64_t)1 << 17, ((B + 3) / 4 + 4095) / 4096 * 4096);
+    // chunks: about a sixth of the shots each, at least 64 Ki shots
+    const int64_t chunk = std::max<int64_t>((int64_t)1 << 16, ((B + 5) / 6 + 4095) / 4096 * 4096);
     const int n_chunks = (int)((B + chunk - 1) / chunk);
     std::vector<cudaEvent_t> ev_in(n_chunks, nullptr), ev_done(n_chunks, nullptr);
     ksim_status st = KSIM_OK;

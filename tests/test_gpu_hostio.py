@@ -39,7 +39,7 @@ def _device_once(sampler, f, seed, mode):
     return d_out.cpu().numpy()
 
 
-@pytest.mark.parametrize("B", [1, 1000, 131072, 131073, 700_001])
+@pytest.mark.parametrize("B", [1, 1000, 65536, 65537, 131073, 700_001])
 def test_chunked_host_call_equals_one_launch(cuda_device, oracle_port, small_prog, B):
     from ksim_b200.sampler import B200ProgramSampler
     rng, prog, n_f = small_prog
@@ -49,7 +49,7 @@ def test_chunked_host_call_equals_one_launch(cuda_device, oracle_port, small_pro
         got = s.sample(f, 31 + B, rng_mode=mode)
         assert np.array_equal(got, _device_once(s, f, 31 + B, mode)), mode
     # spot-check against the oracle at the chunk seams
-    for lo in sorted({0, max(0, B - 300), min(B, 131072) - 150}):
+    for lo in sorted({0, max(0, B - 300), max(0, min(B, 65536) - 150), max(0, min(B, 131072) - 150)}):
         lo = max(lo, 0)
         hi = min(B, lo + 300)
         want = oracle_port.program_sample(prog, f[lo:hi], 31 + B, rng_mode=1, shot_offset=lo)
