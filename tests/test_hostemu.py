@@ -203,3 +203,26 @@ def test_nodephases_by_sign_counts(hostemu, oracle_port, Tnp):
         dead += int(((want[..., :4] == 0).all(-1) & (want[..., 4] > 0)).sum())
     if Tnp >= 7:
         assert dead > 0
+
+
+@pytest.mark.parametrize("zero", ["alpha", "beta", "both"])
+def test_phasepairs_with_a_zero_rotation(hostemu, oracle_port, zero):
+    """PhasePairs columns with rotation class 0 on one side (1 + a + b - ab is
+    2 or 2b: a select and one halving) give the reference's numerators,
+    on every term path and for terms killed earlier."""
+    rng = np.random.default_rng({"alpha": 11, "beta": 12, "both": 13}[zero])
+    gs = []
+    for k in range(3):
+        g = synth.random_graph(rng, 24, 16 + k, 12, 2, 2, 16)
+        if zero in ("alpha", "both"):
+            g.ph_alpha[:] = g.ph_alpha & 4          # class 0, sign bit kept
+        if zero in ("beta", "both"):
+            g.ph_beta[:] = g.ph_beta & 4
+        gs.append(g)
+    he = HostEmu(hostemu, gs, 16)
+    po = oracle_port.PortOracle(gs, 16)
+    for gi, g in enumerate(gs):
+        pv = rng.integers(0, 2, size=(48, g.np_params.shape[2])).astype(np.uint8)
+        want = po.eval_terms(gi, pv)
+        assert np.array_equal(he.eval_terms(gi, pv), want), gi
+        assert np.array_equal(he.eval_terms(gi, pv, pairs=True), want), gi
