@@ -18,7 +18,7 @@ namespace ksim {
 
 namespace {
 
-template <int W, bool STAGED>
+template <int W, bool STAGED, int PATHS = PATHS_ALL>
 __global__ void __launch_bounds__(256, KSIM_SAMPLE_MIN_CTAS) k_sample(const SampleJob j)
 {
     extern __shared__ __align__(128) uint8_t smem[];
@@ -28,7 +28,8 @@ __global__ void __launch_bounds__(256, KSIM_SAMPLE_MIN_CTAS) k_sample(const Samp
     uint32_t g = 0;
     constexpr int S = shots_per_thread(W);
     uint8_t *scratch = STAGED ? slots + (size_t)NSLOT * j.slot_bytes : slots;
-    sample_tile<W, STAGED, false, S>(j, (int64_t)blockIdx.x * blockDim.x * S, bar, slots, g, scratch);
+    sample_tile<W, STAGED, false, S, PATHS>(j, (int64_t)blockIdx.x * blockDim.x * S, bar, slots, g,
+                                                   scratch);
 }
 
 template <int W>
@@ -84,7 +85,17 @@ cudaError_t launch_sample_w(const SampleJob &j, const LaunchCfg &cfg, cudaStream
     const int64_t blocks = (j.B + tile - 1) / tile;
     if (blocks > 0x7FFFFFFF) return cudaErrorInvalidConfiguration;
     const size_t smem = sample_smem_bytes(j.slot_bytes, cfg.staged != 0, W, threads);
-    if (cfg.staged) {
+    if (cfg.staged && cfg.paths == PATHS_NARROW && W <= 4) {
+        cudaError_t e = cudaFuncSetAttribute(k_sample<W, true, PATHS_NARROW>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        k_sample<W, true, PATHS_NARROW><<<(unsigned)blocks, threads, smem, st>>>(j);
+    } else if (cfg.staged && cfg.paths == PATHS_NARROW_HYBRID && W <= 4) {
+        cudaError_t e = cudaFuncSetAttribute(k_sample<W, true, PATHS_NARROW_HYBRID>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        k_sample<W, true, PATHS_NARROW_HYBRID><<<(unsigned)blocks, threads, smem, st>>>(j);
+    } else if (cfg.staged) {
         cudaError_t e = cudaFuncSetAttribute(k_sample<W, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return e;

@@ -56,6 +56,8 @@ struct LaunchCfg {
     int threads = 256;   // shots per CTA (one shot per thread)
     int staged = 1;      // stage term chunks in shared memory with TMA bulk copies
     int slot_bytes = 16384;
+    int paths = 0;       // term paths the program uses: 0 all, 1 32-bit only, 2 32-bit and hybrid
+                         // (the kernels compiled without the others)
 };
 
 // Launch the plain (one component per launch) sampler.

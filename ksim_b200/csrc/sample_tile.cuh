@@ -228,7 +228,11 @@ __device__ __noinline__ void eval_term_exact_call(const uint8_t *p, const TermHd
 // to (sum_re[s], sum_im[s]) in order (the warp-sliced form of eval_terms_s).
 // sw: the warp's ballot words; wb: this thread's row-parity words (block b,
 // shot r at wb[b * S * blockDim + r * blockDim]).
-template <int W, int S>
+// PATHS: which term paths the program uses (the host checked), so the others
+// are not compiled in: PATHS_ALL, PATHS_NARROW (every term on 32-bit words),
+// PATHS_NARROW_HYBRID (32-bit words and the hybrid path).
+enum : int { PATHS_ALL = 0, PATHS_NARROW = 1, PATHS_NARROW_HYBRID = 2 };
+template <int W, int S, int PATHS = PATHS_ALL>
 __device__ __forceinline__ const uint8_t *eval_terms_warp(const uint8_t *p, uint32_t n_terms,
                                                           const uint64_t (&v)[S][W], const uint8_t *sw,
                                                           uint32_t *wb, double (&sum_re)[S], double (&sum_im)[S],
@@ -238,7 +242,7 @@ __device__ __forceinline__ const uint8_t *eval_terms_warp(const uint8_t *p, uint
     for (uint32_t t = 0; t < n_terms; ++t) {
         const TermHdr h = load_hdr(p);
         TermOut o[S];
-        if (h.flags & TF_SLOW) {
+        if (PATHS == PATHS_ALL && (h.flags & TF_SLOW)) {
 #pragma unroll
             for (int s = 0; s < S; ++s) eval_term_exact_call<W>(p, h, v[s], o[s]);
         } else {
@@ -277,7 +281,16 @@ __device__ __forceinline__ const uint8_t *eval_terms_warp(const uint8_t *p, uint
                 bits[s].w = wb + s * nt;
                 bits[s].stride = wstride;
             }
-            eval_term_rows_any<S>(p, h, sums, bits, o);
+            if (PATHS == PATHS_NARROW)
+                eval_term_rows<uint32_t, uint32_t, S>(p, h, sums, bits, o);
+            else if (PATHS == PATHS_NARROW_HYBRID) {
+                if (h.flags & TF_NARROW)
+                    eval_term_rows<uint32_t, uint32_t, S>(p, h, sums, bits, o);
+                else
+                    eval_term_rows<uint32_t, uint64_t, S>(p, h, sums, bits, o);
+            } else {
+                eval_term_rows_any<S>(p, h, sums, bits, o);
+            }
         }
 #pragma unroll
         for (int s = 0; s < S; ++s) {
@@ -324,7 +337,7 @@ __device__ __forceinline__ void issue_chunk(const SampleJob &j, int c, uint32_t 
 // count (advanced by the job's chunk count).  Returns false after a wait
 // timeout (the CTA must then stop using the ring).
 // scratch: sliced_smem_bytes(W, blockDim.x) bytes of shared memory.
-template <int W, bool STAGED, bool CG = false, int S = 1>
+template <int W, bool STAGED, bool CG = false, int S = 1, int PATHS = PATHS_ALL>
 __device__ __forceinline__ bool sample_tile(const SampleJob &j, const int64_t s0, uint64_t *bar, uint8_t *slots,
                                             uint32_t &g, uint8_t *scratch)
 {
@@ -406,7 +419,7 @@ __device__ __forceinline__ bool sample_tile(const SampleJob &j, const int64_t s0
         } else {
             p = j.image + d.off;
         }
-        if (warp_any) eval_terms_warp<W, S>(p, (uint32_t)d.n_terms, vk, (const uint8_t *)sw, wb, sre, sim, risk,
+        if (warp_any) eval_terms_warp<W, S, PATHS>(p, (uint32_t)d.n_terms, vk, (const uint8_t *)sw, wb, sre, sim, risk,
                                             live, lane);
         if (d.end_of_graph) {
             const int k = d.graph;
