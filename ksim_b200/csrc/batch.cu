@@ -29,7 +29,7 @@ namespace ksim {
 
 struct BatchJobDev {
     SampleJob j;
-    int32_t W, pad0;
+    int32_t W, paths;  // paths: the component's term paths (LaunchCfg::paths)
     int64_t pad1;
 };
 
@@ -67,12 +67,20 @@ __global__ void __launch_bounds__(256, CLASS == 0 ? KSIM_SAMPLE_MIN_CTAS : 1) k_
         const BatchJobDev &J = jobs[w.job];
         bool ok = true;
         if (CLASS == 0) {
+            // programs whose terms all run on 32-bit words take the kernel
+            // body compiled without the other paths
+#define KSIM_BATCH_W(WW)                                                                                  \
+    case WW:                                                                                              \
+        ok = J.paths == PATHS_NARROW                                                                      \
+                 ? sample_tile<WW, true, false, shots_per_thread(WW), PATHS_NARROW>(J.j, w.s0, bar, slots, g, \
+                                                                                   scratch)               \
+                 : sample_tile<WW, true, false, shots_per_thread(WW)>(J.j, w.s0, bar, slots, g, scratch); \
+        break;
             switch (J.W) {
-            case 1: ok = sample_tile<1, true, false, shots_per_thread(1)>(J.j, w.s0, bar, slots, g, scratch); break;
-            case 2: ok = sample_tile<2, true, false, shots_per_thread(2)>(J.j, w.s0, bar, slots, g, scratch); break;
-            case 3: ok = sample_tile<3, true, false, shots_per_thread(3)>(J.j, w.s0, bar, slots, g, scratch); break;
-            default: ok = sample_tile<4, true, false, shots_per_thread(4)>(J.j, w.s0, bar, slots, g, scratch); break;
+            KSIM_BATCH_W(1) KSIM_BATCH_W(2) KSIM_BATCH_W(3)
+            default: KSIM_BATCH_W(4)
             }
+#undef KSIM_BATCH_W
         } else {
             switch (J.W) {
             case 5: ok = sample_tile<5, true, false, shots_per_thread(5)>(J.j, w.s0, bar, slots, g, scratch); break;
@@ -194,6 +202,7 @@ ksim_status ksim_batch_create(const ksim_batch_job *jobs, int32_t n_jobs, const 
         d.j.shot_offset = jb.shot_offset;
         d.j.seed = jb.seed;
         d.W = c->img.W;
+        d.paths = c->cfg.paths;
         b->host_jobs.push_back(d);
         b->comps.push_back(c);
         if (c->img.n_out == 0 || jb.B == 0) continue;
