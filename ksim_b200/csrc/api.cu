@@ -171,10 +171,12 @@ ksim_status ksim_component_create(const ksim_graph_desc *graphs, int32_t n_graph
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
     // default launch shape: slot fits the largest term and at least 16 KiB;
     // staging is skipped when two slots would not fit in shared memory
-    const int64_t slot = std::max<int64_t>(16384, (c->img.max_term_bytes + 15) & ~int64_t(15));
-    c->cfg.threads = 128;  // 4 CTAs of 128 per SM: a quarter of the warps per barrier
     c->cfg.paths = c->img.n_narrow_terms == c->img.n_terms ? 1
                    : c->img.n_narrow_terms + c->img.n_hybrid_terms == c->img.n_terms ? 2 : 0;
+    // 12 KiB slots for the all-32-bit kernel (five CTAs per SM), 16 KiB else
+    const int64_t slot = std::max<int64_t>(c->cfg.paths == 1 ? 12288 : 16384,
+                                           (c->img.max_term_bytes + 15) & ~int64_t(15));
+    c->cfg.threads = 128;  // CTAs of 128: a quarter of the warps per barrier
     c->cfg.slot_bytes = (int)std::min<int64_t>(slot, 1 << 30);
     c->cfg.staged =
         sample_smem_bytes((int)std::min<int64_t>(slot, 1 << 20), true, c->img.W, c->cfg.threads) <= 200 * 1024 ? 1
