@@ -18,9 +18,10 @@ namespace ksim {
 
 namespace {
 
-// The all-32-bit kernel fits 96 registers: with 128-thread CTAs and 12 KiB
-// staging slots, five CTAs per SM.  The others keep the two-of-256 budget.
-#define KSIM_SAMPLE_BOUNDS(P) __maxnreg__((P) == PATHS_NARROW ? 96 : 65536 / (256 * KSIM_SAMPLE_MIN_CTAS))
+// The kernels without the exact and 64-bit paths fit 96 registers: with
+// 128-thread CTAs and 12 KiB staging slots, five CTAs per SM.  The general
+// kernel keeps the two-of-256 budget.
+#define KSIM_SAMPLE_BOUNDS(P) __maxnreg__((P) != PATHS_ALL ? 96 : 65536 / (256 * KSIM_SAMPLE_MIN_CTAS))
 template <int W, bool STAGED, int PATHS = PATHS_ALL>
 __global__ void KSIM_SAMPLE_BOUNDS(PATHS) k_sample(const SampleJob j)
 {
