@@ -254,3 +254,26 @@ def test_hybrid_and_wide_terms_on_gpu(cuda_device, oracle_port, Tnp, Tph):
         want, want_amp = po.sample(f, 99, mode, return_amp=True)
         bits, amp = device_sample(kc, f, 99, mode)
         assert np.array_equal(bits, want[:, :kc.n_out]) and same_bits(amp, want_amp)
+
+
+@pytest.mark.parametrize("Tnp,Tph,seed,kind", [(40, 12, 2, "narrow"), (50, 16, 5, "narrow+hybrid"),
+                                                (60, 10, 4, "all")])
+def test_kernel_per_term_path_set(cuda_device, oracle_port, Tnp, Tph, seed, kind):
+    """The plain sampler runs a kernel compiled for the term paths a component
+    uses (every term on 32-bit words; 32-bit and hybrid; any): each equals the
+    oracle, bits and |A_k|, for both uniform streams and for a shot offset."""
+    from ksim_b200.perfmodel import component_work
+    rng = np.random.default_rng(seed)
+    gs = [synth.random_graph(rng, 6, 20 + k, Tnp, 3, 3, Tph) for k in range(4)]
+    comp = FlatComponent((0, 1, 2), np.arange(20, dtype=np.int32), gs)
+    w = component_work(comp)
+    got_kind = ("narrow" if w["hybrid_terms"] + w["wide_terms"] + w["exact_terms"] == 0 else
+                "narrow+hybrid" if w["wide_terms"] + w["exact_terms"] == 0 else "all")
+    assert got_kind == kind, w
+    kc = _component(comp.graphs, 20)
+    po = oracle_port.PortOracle(comp.graphs, 20)
+    f = synth.sample_f(rng, 3000, 20, 0.1)
+    for mode, off in ((0, 0), (1, 0), (1, 777)):
+        want, want_amp = po.sample(f, 123, mode, return_amp=True, shot_offset=off)
+        bits, amp = device_sample(kc, f, 123, mode, shot_offset=off)
+        assert np.array_equal(bits, want[:, :kc.n_out]) and same_bits(amp, want_amp), (mode, off)
