@@ -119,15 +119,14 @@ bool all_zero(const uint64_t *m, int W)
 //     transposes: 2 x 5 rounds x 2 (rotate, select) x 32 lanes / 64 = 10
 //     block sums: 4 (and) + 4 (popcount) + 1 (shift) + 4 (accumulate) = 13
 //   NodePhases: C * lambda^e, 16 multiply-adds x c_np + 4 (mask) + 2
-//   PhasePairs with a rotation 0: 3 (bits) + 2 (sign) + 4c (signed copy)
-//               + 4c (select) + 4 (zero test, pw)
-//   other PhasePairs: 3 (bits) + 3 (signs) + 12c (three rotated adds)
-//               + 4 (evenness) + 4c + 1 (conditional halving)
+//   PhasePairs, per pair of columns: 3 (sign bits) + 6 (valuations) + 8
+//               (two halving decisions) + 8 (factor read and unpack) + 16c
+//               (product) + 4c + 1 (shift, pw); an odd last column: 3 + 3 +
+//               12c (three rotated adds) + 4 (evenness) + 4c + 1
 //   per term: ff * w^k read 4, floatfactor product 16 (c = 1) or 64 (c = 2),
 //             renormalisation 6c, complex value and sum 16
 //   per graph: parameter vector 4W + 8, ballot words 4, Bernoulli step 10
-double term_work(int W, uint32_t flags, const int n_cls[4], int n_hp, int n_pp, int n_ph, int n_ph_unit, int nb,
-                 int sum_iter)
+double term_work(int W, uint32_t flags, const int n_cls[4], int n_hp, int n_pp, int n_ph, int nb, int sum_iter)
 {
     const double par = 3.0 * W + 2.0;
     const int n_np = n_cls[0] + n_cls[1] + n_cls[2] + n_cls[3];
@@ -138,8 +137,8 @@ double term_work(int W, uint32_t flags, const int n_cls[4], int n_hp, int n_pp, 
     double w = (double)sum_iter + 23.0 * nb;
     if (n_cls[1] | n_cls[3]) w += 16.0 * cn + 2.0;
     w += 4.0 * cn;
-    w += n_ph_unit * (3.0 + 2.0 + 8.0 * c + 4.0);
-    w += (n_ph - n_ph_unit) * (3.0 + 3.0 + 12.0 * c + 4.0 + 4.0 * c + 1.0);
+    w += (n_ph / 2) * (3.0 + 6.0 + 8.0 + 8.0 + 16.0 * c + 4.0 * c + 1.0);
+    w += (n_ph & 1) * (3.0 + 3.0 + 12.0 * c + 4.0 + 4.0 * c + 1.0);
     w += 4.0 + (c == 1.0 ? 16.0 : 64.0) + 6.0 * c + 16.0;
     return w;
 }
@@ -284,10 +283,6 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             double ref_max = 0, fast_max = 0;
             const double kLim = 62.0 - 1e-9;
             bool unsafe = false;
-            auto step = [&](double v) {
-                ref_max = std::max(ref_max, v);
-                fast_max = std::max(fast_max, v);
-            };
             // NodePhases.  A column's mask carries the constant bit iff bit 2
             // of its phase is set, so its parity is the sign of w^(4 par):
             // factor = 1 + (-1)^parity w^(phase & 3).  Every factor has
@@ -375,8 +370,9 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             // PhasePairs: the bound per valuation of z ((1 - w)-adic; the
             // block's result has nu = the leftover above, for every shot
             // whose term survives)
-            std::map<uint32_t, double> ph_state;
+            std::map<uint32_t, double> ph_state;  // the reference's steps
             ph_state[nu] = L_np;
+            std::vector<std::pair<uint32_t, uint32_t>> ph_j;  // rotation classes (ja, jb) per column
             // HalfPi
             int n_hp = 0;
             for (int c = 0; c < g.Thp; ++c) {
@@ -417,7 +413,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 ++n_pp;
             }
             // PhasePairs
-            int n_ph = 0, n_ph_unit = 0;
+            int n_ph = 0;
             for (int c = 0; c < cph; ++c) {
                 const size_t ci = (size_t)t * g.Tph + c;
                 if (!pack_mask(g.ph_alpha_p + ci * P, P, W, mask.data()) ||
@@ -426,7 +422,6 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                     return KSIM_ERR_MALFORMED_PROGRAM;
                 }
                 const uint32_t ac = g.ph_alpha[ci] & 7u, bc = g.ph_beta[ci] & 7u, gc = (ac + bc) & 7u;
-                if ((ac & 3u) == 0 || (bc & 3u) == 0) ++n_ph_unit;
                 const uint32_t a2 = ac >> 2, b2 = bc >> 2;
                 // the masks carry bit 2 of alpha / beta in the constant bit, so
                 // pa' = pa ^ a2 and pb' = pb ^ b2 are the signs of the w^a and
@@ -447,7 +442,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                     const double lf = std::log2(max_embed(f)) + 1e-12;
                     for (const auto &sv : ph_state) {
                         double x = sv.second + lf;
-                        step(x);
+                        ref_max = std::max(ref_max, x);
                         uint32_t s1 = sv.first + v;
                         if (s1 >= 4) {
                             s1 -= 4;
@@ -458,6 +453,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                     }
                 }
                 ph_state.swap(next);
+                ph_j.push_back({ac & 3u, bc & 3u});
                 ph_rows.push_back({std::vector<uint64_t>(mask.begin(), mask.begin() + W), (uint32_t)cw});
                 ph_rows.push_back({std::vector<uint64_t>(mask.begin() + W, mask.begin() + 2 * W), 0});
                 for (int w = 0; w < 2 * W; ++w) put64(rec, mask[w]);
@@ -471,7 +467,80 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             const double S = std::fabs((double)ff[0]) + std::fabs((double)ff[1]) +
                              std::fabs((double)ff[2]) + std::fabs((double)ff[3]);
             if (S > 0)
-                for (const auto &sv : ph_state) step(sv.second + std::log2(S) + 1e-12);
+                for (const auto &sv : ph_state) ref_max = std::max(ref_max, sv.second + std::log2(S) + 1e-12);
+            // The fast path runs PhasePairs columns in pairs (zring.cuh): its
+            // exact points are the unhalved pair product and, for an odd last
+            // column, the single factor; then the end.  Pair tables: the 16
+            // products F F' and the factors' valuations, by folded signs.
+            auto ph_factor = [&](size_t col, uint32_t k, int64_t f[4]) {
+                phase_pair((int)(ph_j[col].first | ((k & 1u) << 2)), (int)(ph_j[col].second | ((k >> 1) << 2)), f);
+            };
+            const size_t n_pair = (size_t)n_ph / 2;
+            std::vector<uint8_t> pair_tab(64 * n_pair, 0);
+            std::vector<uint32_t> pair_nu(n_pair, 0);
+            bool pair_ok = true;
+            {
+                std::map<uint32_t, double> fs;
+                fs[nu] = L_np;
+                for (size_t q = 0; q < n_pair; ++q) {
+                    for (uint32_t k = 0; k < 4; ++k) {
+                        int64_t f[4];
+                        ph_factor(2 * q, k, f);
+                        pair_nu[q] |= std::min<uint32_t>(zw_valuation(f), 15u) << (4 * k);
+                        ph_factor(2 * q + 1, k, f);
+                        pair_nu[q] |= std::min<uint32_t>(zw_valuation(f), 15u) << (16 + 4 * k);
+                    }
+                    std::map<uint32_t, double> next;
+                    for (uint32_t c = 0; c < 16; ++c) {
+                        int64_t f1[4], f2[4];
+                        ph_factor(2 * q, c & 3u, f1);
+                        ph_factor(2 * q + 1, c >> 2, f2);
+                        const Zu a = {(uint64_t)f1[0], (uint64_t)f1[1], (uint64_t)f1[2], (uint64_t)f1[3]};
+                        const Zu b = {(uint64_t)f2[0], (uint64_t)f2[1], (uint64_t)f2[2], (uint64_t)f2[3]};
+                        const Zu pr = zmul(a, b);
+                        const int64_t pc[4] = {(int64_t)pr.a, (int64_t)pr.b, (int64_t)pr.c, (int64_t)pr.d};
+                        for (int i = 0; i < 4; ++i) {
+                            if (pc[i] < -128 || pc[i] > 127) pair_ok = false;
+                            pair_tab[64 * q + 4 * c + (size_t)i] = (uint8_t)(int8_t)pc[i];
+                        }
+                        const uint32_t v1 = zw_valuation(f1), v2 = zw_valuation(f2);
+                        if (v1 == NU_ZERO || v2 == NU_ZERO) continue;
+                        const double l12 = std::log2(max_embed(pc)) + 1e-12;
+                        for (const auto &sv : fs) {
+                            double x = sv.second + l12;
+                            fast_max = std::max(fast_max, x);
+                            uint32_t s1 = sv.first + v1;
+                            if (s1 >= 4) { s1 -= 4; x -= 1.0; }
+                            s1 += v2;
+                            if (s1 >= 4) { s1 -= 4; x -= 1.0; }
+                            auto it = next.find(s1);
+                            if (it == next.end() || it->second < x) next[s1] = x;
+                        }
+                    }
+                    fs.swap(next);
+                }
+                if (n_ph & 1) {
+                    std::map<uint32_t, double> next;
+                    for (uint32_t k = 0; k < 4; ++k) {
+                        int64_t f[4];
+                        ph_factor((size_t)n_ph - 1, k, f);
+                        const uint32_t v = zw_valuation(f);
+                        if (v == NU_ZERO) continue;
+                        const double lf = std::log2(max_embed(f)) + 1e-12;
+                        for (const auto &sv : fs) {
+                            double x = sv.second + lf;
+                            fast_max = std::max(fast_max, x);
+                            uint32_t s1 = sv.first + v;
+                            if (s1 >= 4) { s1 -= 4; x -= 1.0; }
+                            auto it = next.find(s1);
+                            if (it == next.end() || it->second < x) next[s1] = x;
+                        }
+                    }
+                    fs.swap(next);
+                }
+                if (S > 0)
+                    for (const auto &sv : fs) fast_max = std::max(fast_max, sv.second + std::log2(S) + 1e-12);
+            }
             if (n_np > 0xFFFF || n_hp > 0xFFFF || n_pp > 0xFFFF || n_ph > 0xFFFF) {
                 err = gname + ": a term has more than 65535 columns in one family";
                 return KSIM_ERR_UNSUPPORTED;
@@ -487,7 +556,8 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             // 32-bit negative)
             bool ff_min = false;
             for (int i = 0; i < 4; ++i) ff_min |= ff[i] == INT32_MIN;
-            if (ref_max > kLim || std::max(n_cls[1], n_cls[3]) > LAM_MAX || !c_ok || max_dead > 0xFFFFu || ff_min)
+            if (ref_max > kLim || fast_max > kLim || !pair_ok || std::max(n_cls[1], n_cls[3]) > LAM_MAX || !c_ok ||
+                max_dead > 0xFFFFu || ff_min)
                 unsafe = true;
             uint32_t flags = unsafe ? TF_SLOW : (fast_max <= 30.5 ? TF_NARROW : (L_np <= 30.5 ? TF_HYBRID : 0u));
             // the fast paths' parity rows (row order and block masks:
@@ -514,6 +584,10 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 for (size_t i = 0; i < pair_rows.size(); ++i) {
                     rows.push_back(&pair_rows[i].m);
                     role.push_back((i & 1u) ? 0u : R_PP);
+                }
+                while (rows.size() & 3u) {  // PhasePairs pairs: 4-bit aligned
+                    rows.push_back(&zero_row);
+                    role.push_back(0u);
                 }
                 for (const Row &q : ph_rows) {
                     rows.push_back(&q.m);
@@ -554,6 +628,9 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                         body.push_back((uint8_t)(d >> 8));
                     }
                 for (size_t i = 0; i < ph_rows.size(); i += 2) body.push_back((uint8_t)ph_rows[i].c);
+                while (body.size() & 15u) body.push_back(0);
+                body.insert(body.end(), pair_tab.begin(), pair_tab.end());
+                for (uint32_t v : pair_nu) put32(body, v);
                 while (body.size() & 15u) body.push_back(0);
                 nb = (uint32_t)((rows.size() + 31) / 32);
                 const uint16_t zero_off = (uint16_t)(8 * 64 * W);
@@ -622,7 +699,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             img.n_narrow_terms += (flags & TF_NARROW) ? 1 : 0;
             img.n_hybrid_terms += (flags & TF_HYBRID) ? 1 : 0;
             img.n_columns += n_np + n_hp + n_pp + n_ph;
-            img.work_ops += term_work(W, flags, n_cls, n_hp, n_pp, n_ph, n_ph_unit, (int)nb, (int)sum_iter);
+            img.work_ops += term_work(W, flags, n_cls, n_hp, n_pp, n_ph, (int)nb, (int)sum_iter);
         }
         toff.push_back((int64_t)out.size());
         img.work_ops += graph_work(W);

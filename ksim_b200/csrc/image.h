@@ -46,8 +46,7 @@ int build_image(const ksim_graph_desc *graphs, int n_graphs, int F, HostImage &o
 
 // int32 operations of one shot for one term / one graph (the roofline
 // numerator; see image.cpp).
-double term_work(int W, uint32_t flags, const int n_cls[4], int n_hp, int n_pp, int n_ph, int n_ph_unit, int nb,
-                 int sum_iter);
+double term_work(int W, uint32_t flags, const int n_cls[4], int n_hp, int n_pp, int n_ph, int nb, int sum_iter);
 double graph_work(int W);
 
 // Split every graph's term stream into chunks of whole terms of at most

@@ -456,13 +456,15 @@ KS_HD void ph_unit(Zr<T> &z, uint32_t psel, uint32_t psign, int32_t &pw)
 // A fast term's columns are parity rows over the parameter vector, each
 // stored as the list of its set bits.  Row order (term-relative position):
 //   NodePhases class 0, 2, 1, 3 | HalfPi | (a zero row if needed to make the
-//   next position even) | PiProducts (psi, phi) pairs | PhasePairs (alpha,
-//   beta) pairs
+//   next position even) | PiProducts (psi, phi) pairs | (zero rows to a
+//   multiple of 4) | PhasePairs (alpha, beta) pairs
 // After the header (and approximation) the term's constants: the floatfactor
 // times w^(k + phase index) for k = 0..7 (8 x 4 i32, so the final rotation
 // and the floatfactor are one table read and one product), u16 dead_pw per
 // class-0 row, u8 word (ja | K<<2 | jb<<3 | jg<<5) per PhasePairs column,
-// padded to 16 bytes; then nb blocks of 32 rows, each a 32-byte head
+// padded to 16 bytes; the PhasePairs pair tables and valuation words (see
+// term_pair_tab_off), each part padded to 16 bytes; then nb blocks of 32
+// rows, each a 32-byte head
 //   u32 n_pairs, u32 masks P1, P2, P4, E3, E1, PP, K0 (bit i = row 32b + i)
 // and n_pairs x 32 u32 words of two u16 byte offsets (8 x bit index; word
 // [i][r] holds the set bits 2i and 2i + 1 of row r of the block, 8 x 64W,
@@ -478,9 +480,18 @@ KS_HD void ph_unit(Zr<T> &z, uint32_t psel, uint32_t psign, int32_t &pw)
 constexpr int BLOCK_HEAD_BYTES = 32;
 KS_HD int term_meta_off(const TermHdr &h) { return TERM_HDR_BYTES + ((h.flags & TF_APX) ? TERM_APX_BYTES : 0); }
 constexpr int TERM_FFK_BYTES = 128;
-KS_HD int term_blocks_off(const TermHdr &h)
+// PhasePairs columns 2p and 2p + 1 (p < n_ph / 2) run as one pair: a table of
+// their 16 products (4 x i8 each, combo = pa | pb << 1 | pa' << 2 | pb' << 3)
+// and a word of the two factors' (1 - w)-adic valuations per sign pair
+// (nibble k = factor 1 for pa | pb << 1 = k, nibble 4 + k = factor 2; 15 = 0).
+KS_HD int term_pair_tab_off(const TermHdr &h)
 {
     return term_meta_off(h) + TERM_FFK_BYTES + ((2 * (int)h.n_cls[0] + (int)h.n_ph + 15) & ~15);
+}
+KS_HD int term_pair_nu_off(const TermHdr &h) { return term_pair_tab_off(h) + 64 * (int)(h.n_ph >> 1); }
+KS_HD int term_blocks_off(const TermHdr &h)
+{
+    return term_pair_nu_off(h) + ((4 * (int)(h.n_ph >> 1) + 15) & ~15);
 }
 KS_HD void load_i32x4(const uint8_t *p, int32_t (&r)[4])
 {
@@ -496,7 +507,7 @@ KS_HD void load_i32x4(const uint8_t *p, int32_t (&r)[4])
 KS_HD int term_ph_row0(const TermHdr &h)
 {
     const int pp0 = ((int)(h.n_np + h.n_hp) + 1) & ~1;
-    return pp0 + 2 * (int)h.n_pp;
+    return (pp0 + 2 * (int)h.n_pp + 3) & ~3;  // pairs of PhasePairs columns: 4-bit aligned
 }
 
 KS_HD uint32_t popc32(uint32_t x)
@@ -649,12 +660,45 @@ KS_HD const uint8_t *eval_term_rows(const uint8_t *p, const TermHdr &h, const Ro
         }
     }
     const int ph0 = term_ph_row0(h);
-    // PhasePairs: after each factor the reference's renormalisation step,
-    // halve once if all four coefficients are even and not all zero
-    // (zx_eval.hpp:35-41).  z here differs from the reference's by a unit
-    // (the NodePhases form, the deferred rotations), and units preserve
-    // evenness, so every decision is the reference's.
-    for (uint32_t t = 0; t < h.n_ph; ++t) {
+    // PhasePairs in pairs: the valuation of z (known per shot: the
+    // NodePhases result has nu = (2 n2 + n1 + n3) mod 4, and each factor's nu
+    // is tabulated) decides the reference's two halvings, so one product
+    // with the tabulated F F' and one shift replace two factors and two
+    // evenness tests.  A zero factor leaves z = 0 and no halving after it.
+    {
+        const uint32_t n_pair = h.n_ph >> 1;
+        const uint8_t *ptab = p + term_pair_tab_off(h);
+        const uint32_t *pnu = (const uint32_t *)(p + term_pair_nu_off(h));
+        uint32_t nu[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) nu[s] = (2u * h.n_cls[1] + h.n_cls[2] + h.n_cls[3]) & 3u;
+        for (uint32_t q = 0; q < n_pair; ++q) {
+            const uint32_t nuw = pnu[q];
+            const int pos = ph0 + 4 * (int)q;
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const uint32_t c = (bits[s].word(pos >> 5) >> (pos & 31)) & 15u;
+                const uint32_t v1 = (nuw >> (4u * (c & 3u))) & 15u, v2 = (nuw >> (16u + 4u * (c >> 2))) & 15u;
+                // a zero factor stops the halvings from where it acts: the
+                // first factor's halving still happens if only the second is 0
+                alive[s] &= v1 != 15u ? 1u : 0u;
+                uint32_t t = nu[s] + v1;
+                const uint32_t h1 = (t >= 4u ? 1u : 0u) & alive[s];
+                alive[s] &= v2 != 15u ? 1u : 0u;
+                t = t - 4u * h1 + v2;
+                const uint32_t h2 = (t >= 4u ? 1u : 0u) & alive[s];
+                nu[s] = t - 4u * h2;
+                const uint32_t fw = *(const uint32_t *)(ptab + 64 * q + 4 * c);  // 4 x i8
+                const Zr<T> F = {(T)(int64_t)((int32_t)(fw << 24) >> 24), (T)(int64_t)((int32_t)(fw << 16) >> 24),
+                                 (T)(int64_t)((int32_t)(fw << 8) >> 24), (T)(int64_t)((int32_t)fw >> 24)};
+                z[s] = zmul(z[s], F);
+                shr_all(z[s], h1 + h2);
+                pw[s] += (int32_t)(h1 + h2);
+            }
+        }
+    }
+    // an odd last column alone, with the reference's evenness test
+    for (uint32_t t = h.n_ph & ~1u; t < h.n_ph; ++t) {
         const uint32_t cw = ph_cw[t];
         const uint32_t K = (cw >> 2) & 1u;
         uint32_t pa[S], pb[S];
