@@ -119,10 +119,9 @@ bool all_zero(const uint64_t *m, int W)
 //     transposes: 2 x 5 rounds x 2 (rotate, select) x 32 lanes / 64 = 10
 //     block sums: 4 (and) + 4 (popcount) + 1 (shift) + 4 (accumulate) = 13
 //   NodePhases: C * lambda^e, 16 multiply-adds x c_np + 4 (mask) + 2
-//   PhasePairs, per pair of columns: 3 (sign bits) + 6 (valuations) + 8
-//               (two halving decisions) + 8 (factor read and unpack) + 16c
-//               (product) + 4c + 1 (shift, pw); an odd last column: 3 + 3 +
-//               12c (three rotated adds) + 4 (evenness) + 4c + 1
+//   PhasePairs, per pair of columns (an odd last one pairs with 1): 3 (sign
+//               bits) + 6 (valuations) + 8 (two halving decisions) + 8 (factor
+//               read and unpack) + 16c (product) + 4c + 1 (shift, pw)
 //   per term: ff * w^k read 4, floatfactor product 16 (c = 1) or 64 (c = 2),
 //             renormalisation 6c, complex value and sum 16
 //   per graph: parameter vector 4W + 8, ballot words 4, Bernoulli step 10
@@ -137,8 +136,7 @@ double term_work(int W, uint32_t flags, const int n_cls[4], int n_hp, int n_pp, 
     double w = (double)sum_iter + 23.0 * nb;
     if (n_cls[1] | n_cls[3]) w += 16.0 * cn + 2.0;
     w += 4.0 * cn;
-    w += (n_ph / 2) * (3.0 + 6.0 + 8.0 + 8.0 + 16.0 * c + 4.0 * c + 1.0);
-    w += (n_ph & 1) * (3.0 + 3.0 + 12.0 * c + 4.0 + 4.0 * c + 1.0);
+    w += ((n_ph + 1) / 2) * (3.0 + 6.0 + 8.0 + 8.0 + 16.0 * c + 4.0 * c + 1.0);
     w += 4.0 + (c == 1.0 ? 16.0 : 64.0) + 6.0 * c + 16.0;
     return w;
 }
@@ -469,32 +467,39 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             if (S > 0)
                 for (const auto &sv : ph_state) ref_max = std::max(ref_max, sv.second + std::log2(S) + 1e-12);
             // The fast path runs PhasePairs columns in pairs (zring.cuh): its
-            // exact points are the unhalved pair product and, for an odd last
-            // column, the single factor; then the end.  Pair tables: the 16
+            // exact points are the unhalved pair products, then the end.  Pair tables: the 16
             // products F F' and the factors' valuations, by folded signs.
             auto ph_factor = [&](size_t col, uint32_t k, int64_t f[4]) {
                 phase_pair((int)(ph_j[col].first | ((k & 1u) << 2)), (int)(ph_j[col].second | ((k >> 1) << 2)), f);
             };
-            const size_t n_pair = (size_t)n_ph / 2;
+            // (an odd last column pairs with the factor 1: valuation 0)
+            const size_t n_pair = ((size_t)n_ph + 1) / 2;
             std::vector<uint8_t> pair_tab(64 * n_pair, 0);
             std::vector<uint32_t> pair_nu(n_pair, 0);
             bool pair_ok = true;
+            auto ph_factor2 = [&](size_t col, uint32_t k, int64_t f[4]) {
+                if (col < (size_t)n_ph) {
+                    ph_factor(col, k, f);
+                } else {
+                    f[0] = 1; f[1] = 0; f[2] = 0; f[3] = 0;
+                }
+            };
             {
                 std::map<uint32_t, double> fs;
                 fs[nu] = L_np;
                 for (size_t q = 0; q < n_pair; ++q) {
                     for (uint32_t k = 0; k < 4; ++k) {
                         int64_t f[4];
-                        ph_factor(2 * q, k, f);
+                        ph_factor2(2 * q, k, f);
                         pair_nu[q] |= std::min<uint32_t>(zw_valuation(f), 15u) << (4 * k);
-                        ph_factor(2 * q + 1, k, f);
+                        ph_factor2(2 * q + 1, k, f);
                         pair_nu[q] |= std::min<uint32_t>(zw_valuation(f), 15u) << (16 + 4 * k);
                     }
                     std::map<uint32_t, double> next;
                     for (uint32_t c = 0; c < 16; ++c) {
                         int64_t f1[4], f2[4];
-                        ph_factor(2 * q, c & 3u, f1);
-                        ph_factor(2 * q + 1, c >> 2, f2);
+                        ph_factor2(2 * q, c & 3u, f1);
+                        ph_factor2(2 * q + 1, c >> 2, f2);
                         const Zu a = {(uint64_t)f1[0], (uint64_t)f1[1], (uint64_t)f1[2], (uint64_t)f1[3]};
                         const Zu b = {(uint64_t)f2[0], (uint64_t)f2[1], (uint64_t)f2[2], (uint64_t)f2[3]};
                         const Zu pr = zmul(a, b);
@@ -512,26 +517,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                             uint32_t s1 = sv.first + v1;
                             if (s1 >= 4) { s1 -= 4; x -= 1.0; }
                             s1 += v2;
-                            if (s1 >= 4) { s1 -= 4; x -= 1.0; }
-                            auto it = next.find(s1);
-                            if (it == next.end() || it->second < x) next[s1] = x;
-                        }
-                    }
-                    fs.swap(next);
-                }
-                if (n_ph & 1) {
-                    std::map<uint32_t, double> next;
-                    for (uint32_t k = 0; k < 4; ++k) {
-                        int64_t f[4];
-                        ph_factor((size_t)n_ph - 1, k, f);
-                        const uint32_t v = zw_valuation(f);
-                        if (v == NU_ZERO) continue;
-                        const double lf = std::log2(max_embed(f)) + 1e-12;
-                        for (const auto &sv : fs) {
-                            double x = sv.second + lf;
-                            fast_max = std::max(fast_max, x);
-                            uint32_t s1 = sv.first + v;
-                            if (s1 >= 4) { s1 -= 4; x -= 1.0; }
+                            if (s1 >= 4 && 2 * q + 1 < (size_t)n_ph) { s1 -= 4; x -= 1.0; }
                             auto it = next.find(s1);
                             if (it == next.end() || it->second < x) next[s1] = x;
                         }
@@ -627,7 +613,6 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                         body.push_back((uint8_t)(d & 0xFFu));
                         body.push_back((uint8_t)(d >> 8));
                     }
-                for (size_t i = 0; i < ph_rows.size(); i += 2) body.push_back((uint8_t)ph_rows[i].c);
                 while (body.size() & 15u) body.push_back(0);
                 body.insert(body.end(), pair_tab.begin(), pair_tab.end());
                 for (uint32_t v : pair_nu) put32(body, v);

@@ -397,61 +397,6 @@ struct TermOut {
     uint32_t risk;  // KSIM_FLAG_INT64_RISK raised by the exact path
 };
 
-// One PhasePairs factor 1 + sa w^JA + sb w^JB + sg w^(JA+JB) applied to z,
-// sa = (-1)^pa, sb = (-1)^pb, sg = -(-1)^(K ^ pa ^ pb) (bit 2 of alpha / beta
-// folded into pa / pb; K carries the rest of the -w^(alpha+beta) sign).
-template <typename T, int JA, int JB>
-KS_HD void ph_update(Zr<T> &z, uint32_t pa, uint32_t pb, uint32_t K)
-{
-    constexpr uint32_t JG = (uint32_t)((JA + JB) & 3);
-    const uint32_t pg = K ^ pa ^ pb;
-    const Zr<T> t0 = z;
-    if constexpr (JA == 0 && JB == 0) {
-        // a scalar factor 1 + sa + sb + sg = 4 - 2 (pa + pb + pg)
-        const T f = (T)4 - (T)2 * (T)(pa + pb + pg);
-        z.a = t0.a * f; z.b = t0.b * f; z.c = t0.c * f; z.d = t0.d * f;
-    } else {
-        add_rot(z, t0, (uint32_t)JA, pa);
-        add_rot(z, t0, (uint32_t)JB, pb);
-        add_rot(z, t0, JG, pg);
-    }
-}
-
-// The reference's renormalisation after a PhasePairs factor: halve once if
-// all four coefficients are even and not all zero (zx_eval.hpp:35-41).
-template <typename T>
-KS_HD void ph_halve(Zr<T> &z, int32_t &pw)
-{
-    const T ov = z.a | z.b | z.c | z.d;
-    const uint32_t red = (ov != 0 && (ov & 1u) == 0) ? 1u : 0u;
-    shr_all(z, red);
-    pw += (int32_t)red;
-}
-
-// A PhasePairs factor one of whose rotations is 0: with a = (-1)^psel (that
-// copy) and b = (-1)^psign w^J (the other), 1 + a + b - ab is 2 (psel = 0) or
-// 2b (psel = 1).  The product is even, so the reference halves it once
-// unless z is zero: z becomes z or (-1)^psign R_J(z), and pw grows by one.
-template <typename T, int J>
-KS_HD void ph_unit(Zr<T> &z, uint32_t psel, uint32_t psign, int32_t &pw)
-{
-    const T ov = z.a | z.b | z.c | z.d;
-    pw += ov != 0 ? 1 : 0;
-    const Sign<T> g = sign_of(psign, T());
-    const T p = g.pos, n = g.neg;
-    Zr<T> r;
-    if constexpr (J == 0) {
-        r.a = sadd((T)0, z.a, p); r.b = sadd((T)0, z.b, p); r.c = sadd((T)0, z.c, p); r.d = sadd((T)0, z.d, p);
-    } else if constexpr (J == 1) {
-        r.a = sadd((T)0, z.d, p); r.b = sadd((T)0, z.a, p); r.c = sadd((T)0, z.b, p); r.d = sadd((T)0, z.c, n);
-    } else if constexpr (J == 2) {
-        r.a = sadd((T)0, z.c, n); r.b = sadd((T)0, z.d, p); r.c = sadd((T)0, z.a, p); r.d = sadd((T)0, z.b, n);
-    } else {
-        r.a = sadd((T)0, z.b, n); r.b = sadd((T)0, z.c, n); r.c = sadd((T)0, z.d, p); r.d = sadd((T)0, z.a, n);
-    }
-    if (psel) z = r;
-}
-
 // ---- fast terms: parity rows -------------------------------------------------
 // A fast term's columns are parity rows over the parameter vector, each
 // stored as the list of its set bits.  Row order (term-relative position):
@@ -461,10 +406,9 @@ KS_HD void ph_unit(Zr<T> &z, uint32_t psel, uint32_t psign, int32_t &pw)
 // After the header (and approximation) the term's constants: the floatfactor
 // times w^(k + phase index) for k = 0..7 (8 x 4 i32, so the final rotation
 // and the floatfactor are one table read and one product), u16 dead_pw per
-// class-0 row, u8 word (ja | K<<2 | jb<<3 | jg<<5) per PhasePairs column,
-// padded to 16 bytes; the PhasePairs pair tables and valuation words (see
-// term_pair_tab_off), each part padded to 16 bytes; then nb blocks of 32
-// rows, each a 32-byte head
+// class-0 row, padded to 16 bytes; the PhasePairs pair tables and valuation
+// words (see term_pair_tab_off), each part padded to 16 bytes; then nb
+// blocks of 32 rows, each a 32-byte head
 //   u32 n_pairs, u32 masks P1, P2, P4, E3, E1, PP, K0 (bit i = row 32b + i)
 // and n_pairs x 32 u32 words of two u16 byte offsets (8 x bit index; word
 // [i][r] holds the set bits 2i and 2i + 1 of row r of the block, 8 x 64W,
@@ -480,18 +424,21 @@ KS_HD void ph_unit(Zr<T> &z, uint32_t psel, uint32_t psign, int32_t &pw)
 constexpr int BLOCK_HEAD_BYTES = 32;
 KS_HD int term_meta_off(const TermHdr &h) { return TERM_HDR_BYTES + ((h.flags & TF_APX) ? TERM_APX_BYTES : 0); }
 constexpr int TERM_FFK_BYTES = 128;
-// PhasePairs columns 2p and 2p + 1 (p < n_ph / 2) run as one pair: a table of
-// their 16 products (4 x i8 each, combo = pa | pb << 1 | pa' << 2 | pb' << 3)
-// and a word of the two factors' (1 - w)-adic valuations per sign pair
-// (nibble k = factor 1 for pa | pb << 1 = k, nibble 4 + k = factor 2; 15 = 0).
+// PhasePairs columns 2p and 2p + 1 run as one pair (an odd last column
+// pairs with the factor 1, its sign bits being rows past the end, which are
+// zero): a table of the 16 products (4 x i8 each, combo = pa | pb << 1 |
+// pa' << 2 | pb' << 3) and a word of the two factors' (1 - w)-adic
+// valuations per sign pair (nibble k = factor 1 for pa | pb << 1 = k,
+// nibble 4 + k = factor 2; 15 = the factor is 0).
+KS_HD uint32_t term_ph_pairs(const TermHdr &h) { return (h.n_ph + 1) >> 1; }
 KS_HD int term_pair_tab_off(const TermHdr &h)
 {
-    return term_meta_off(h) + TERM_FFK_BYTES + ((2 * (int)h.n_cls[0] + (int)h.n_ph + 15) & ~15);
+    return term_meta_off(h) + TERM_FFK_BYTES + ((2 * (int)h.n_cls[0] + 15) & ~15);
 }
-KS_HD int term_pair_nu_off(const TermHdr &h) { return term_pair_tab_off(h) + 64 * (int)(h.n_ph >> 1); }
+KS_HD int term_pair_nu_off(const TermHdr &h) { return term_pair_tab_off(h) + 64 * (int)term_ph_pairs(h); }
 KS_HD int term_blocks_off(const TermHdr &h)
 {
-    return term_pair_nu_off(h) + ((4 * (int)(h.n_ph >> 1) + 15) & ~15);
+    return term_pair_nu_off(h) + ((4 * (int)term_ph_pairs(h) + 15) & ~15);
 }
 KS_HD void load_i32x4(const uint8_t *p, int32_t (&r)[4])
 {
@@ -628,7 +575,6 @@ KS_HD const uint8_t *eval_term_rows(const uint8_t *p, const TermHdr &h, const Ro
                                     const RowBits (&bits)[S], TermOut (&o)[S])
 {
     const uint8_t *meta = p + term_meta_off(h);
-    const uint8_t *ph_cw = meta + TERM_FFK_BYTES + 2 * h.n_cls[0];
     uint32_t rot[S], lam[S], alive[S];
     int32_t pw[S];
 #pragma unroll
@@ -666,7 +612,7 @@ KS_HD const uint8_t *eval_term_rows(const uint8_t *p, const TermHdr &h, const Ro
     // with the tabulated F F' and one shift replace two factors and two
     // evenness tests.  A zero factor leaves z = 0 and no halving after it.
     {
-        const uint32_t n_pair = h.n_ph >> 1;
+        const uint32_t n_pair = term_ph_pairs(h);
         const uint8_t *ptab = p + term_pair_tab_off(h);
         const uint32_t *pnu = (const uint32_t *)(p + term_pair_nu_off(h));
         uint32_t nu[S];
@@ -675,6 +621,7 @@ KS_HD const uint8_t *eval_term_rows(const uint8_t *p, const TermHdr &h, const Ro
         for (uint32_t q = 0; q < n_pair; ++q) {
             const uint32_t nuw = pnu[q];
             const int pos = ph0 + 4 * (int)q;
+            const uint32_t second = 2 * q + 1 < h.n_ph ? 1u : 0u;  // the factor 1 takes no step
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 const uint32_t c = (bits[s].word(pos >> 5) >> (pos & 31)) & 15u;
@@ -686,7 +633,7 @@ KS_HD const uint8_t *eval_term_rows(const uint8_t *p, const TermHdr &h, const Ro
                 const uint32_t h1 = (t >= 4u ? 1u : 0u) & alive[s];
                 alive[s] &= v2 != 15u ? 1u : 0u;
                 t = t - 4u * h1 + v2;
-                const uint32_t h2 = (t >= 4u ? 1u : 0u) & alive[s];
+                const uint32_t h2 = (t >= 4u ? 1u : 0u) & alive[s] & second;
                 nu[s] = t - 4u * h2;
                 const uint32_t fw = *(const uint32_t *)(ptab + 64 * q + 4 * c);  // 4 x i8
                 const Zr<T> F = {(T)(int64_t)((int32_t)(fw << 24) >> 24), (T)(int64_t)((int32_t)(fw << 16) >> 24),
@@ -695,47 +642,6 @@ KS_HD const uint8_t *eval_term_rows(const uint8_t *p, const TermHdr &h, const Ro
                 shr_all(z[s], h1 + h2);
                 pw[s] += (int32_t)(h1 + h2);
             }
-        }
-    }
-    // an odd last column alone, with the reference's evenness test
-    for (uint32_t t = h.n_ph & ~1u; t < h.n_ph; ++t) {
-        const uint32_t cw = ph_cw[t];
-        const uint32_t K = (cw >> 2) & 1u;
-        uint32_t pa[S], pb[S];
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            const int pos = ph0 + 2 * (int)t;
-            const uint32_t x = bits[s].word(pos >> 5) >> (pos & 31);
-            pa[s] = x & 1u;
-            pb[s] = (x >> 1) & 1u;
-        }
-        // one branch on the rotation pair; the third rotation is their sum.
-        // A pair with a rotation 0 is a select (ph_unit); the others take the
-        // three rotated adds and the reference's evenness test.
-        switch ((cw & 3u) | ((cw >> 1) & 12u)) {
-#define KSIM_PH_UNIT_A(JB)                                                             \
-    case (JB) << 2:                                                                    \
-        _Pragma("unroll") for (int s = 0; s < S; ++s) ph_unit<T, JB>(z[s], pa[s], pb[s], pw[s]); \
-        break;
-#define KSIM_PH_UNIT_B(JA)                                                             \
-    case (JA):                                                                         \
-        _Pragma("unroll") for (int s = 0; s < S; ++s) ph_unit<T, JA>(z[s], pb[s], pa[s], pw[s]); \
-        break;
-#define KSIM_PH_CASE(JA, JB)                                                           \
-    case (JA) | ((JB) << 2):                                                           \
-        _Pragma("unroll") for (int s = 0; s < S; ++s) {                                \
-            ph_update<T, JA, JB>(z[s], pa[s], pb[s], K);                               \
-            ph_halve(z[s], pw[s]);                                                     \
-        }                                                                              \
-        break;
-        KSIM_PH_UNIT_A(0) KSIM_PH_UNIT_A(1) KSIM_PH_UNIT_A(2) KSIM_PH_UNIT_A(3)
-        KSIM_PH_UNIT_B(1) KSIM_PH_UNIT_B(2) KSIM_PH_UNIT_B(3)
-        KSIM_PH_CASE(1, 1) KSIM_PH_CASE(2, 1) KSIM_PH_CASE(3, 1)
-        KSIM_PH_CASE(1, 2) KSIM_PH_CASE(2, 2) KSIM_PH_CASE(3, 2)
-        KSIM_PH_CASE(1, 3) KSIM_PH_CASE(2, 3) KSIM_PH_CASE(3, 3)
-#undef KSIM_PH_CASE
-#undef KSIM_PH_UNIT_B
-#undef KSIM_PH_UNIT_A
         }
     }
     // prefactor: w^(NodePhases + HalfPi + PiProducts + idx) times the exact
