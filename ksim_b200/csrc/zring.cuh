@@ -7,10 +7,9 @@
 // Multiplying by w^j is a signed rotation of the coefficients:
 //   w^0: ( a,  b,  c,  d)      w^1: ( d,  a,  b, -c)
 //   w^2: (-c,  d,  a, -b)      w^3: (-b, -c,  d, -a)      w^(j+4) = -w^j
-// so every family factor except the floatfactor is a few adds, not a 16-multiply
-// product:
-//   PhasePairs  1 + w^a + w^b - w^(a+b)        ->  z + sa*R(z) + sb*R(z) + sc*R(z)
-//   HalfPi / phase index: a rotation; PiProducts: a sign.
+// HalfPi and the phase index are rotations and PiProducts a sign; the fast
+// path sums them into one rotation, applied with the floatfactor as one
+// product with a tabulated ff * w^k.
 //
 // NodePhases need no per-column arithmetic at all.  A column's factor is
 // 1 + s w^j (s = +-1 from the parity), and 1 - x = (1 + x) u with a unit u:
@@ -29,8 +28,10 @@
 // zx_eval.hpp:35-41) is decided without looking at the coefficients: for
 // nonzero z, all four are even  <=>  nu(z) >= 4, where nu is the
 // (1 - w)-adic valuation (2 = unit * (1 - w)^4), and nu is additive under
-// products.  PhasePairs factors depend on the shot's parities and take the
-// explicit test per shot.  This reproduces the reference's (a, b, c, d, pw)
+// products.  PhasePairs factors 1 + w^a + w^b - w^(a+b) depend on the shot's
+// parities; the host tabulates each factor's nu per sign pair, so a shot
+// tracks nu(z) and runs two columns at a time: their two halving decisions,
+// one product with the tabulated pair product, one shift.  This reproduces the reference's (a, b, c, d, pw)
 // exactly whenever no coefficient leaves the int64 range (all the fast path's
 // arithmetic wraps like the reference's, and only a halving or the end needs
 // the true value); the host proves that per term from an embedding-norm bound
