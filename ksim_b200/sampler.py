@@ -87,17 +87,22 @@ class B200ProgramSampler:
 
 
     def sample_packed(self, f_packed: np.ndarray, n_f_cols: int, seed: int,
-                      rng_mode: int = RNG_XORSHIFT) -> np.ndarray:
+                      rng_mode: int = RNG_XORSHIFT, out: np.ndarray | None = None) -> np.ndarray:
         """``sample`` with bit-packed rows: ``f_packed`` is (B, ceil(n_f_cols/8))
         uint8 as ``np.packbits(f, axis=1, bitorder="little")``; returns
-        (B, ceil(num_outputs/8)) packed the same way."""
+        (B, ceil(num_outputs/8)) packed the same way.  ``out`` (optional): a
+        C-contiguous array of that shape to fill, e.g. page-locked memory."""
         f = np.ascontiguousarray(f_packed, dtype=np.uint8)
         if f.ndim != 2 or f.shape[1] != (int(n_f_cols) + 7) // 8:
             raise ValueError(f"f_packed must have {(int(n_f_cols) + 7) // 8} bytes per row")
         if n_f_cols < self.min_f_cols:
             raise IndexError(f"f_params has {n_f_cols} columns; f_selection needs {self.min_f_cols}")
         B = f.shape[0]
-        out = np.zeros((B, (self.num_outputs + 7) // 8), np.uint8)
+        shape = (B, (self.num_outputs + 7) // 8)
+        if out is None:
+            out = np.zeros(shape, np.uint8)
+        elif out.shape != shape or out.dtype != np.uint8 or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous uint8 array of shape {shape}")
         if B == 0 or self.num_outputs == 0:
             return out
         check(self._L.ksim_program_sample_packed(self._h, _abi.u8ptr(f), B, int(n_f_cols), _as_u64(seed),

@@ -70,8 +70,13 @@ def test_packed_io_equals_byte_io(cuda_device, small_prog, B):
         assert np.array_equal(got, np.packbits(want, axis=1, bitorder="little"))
         unpacked = np.unpackbits(got, axis=1, count=prog.num_outputs, bitorder="little")
         assert np.array_equal(unpacked, want)
+        into = np.full(got.shape, 0xAB, np.uint8)  # a caller's buffer, filled in place
+        assert s.sample_packed(np.packbits(f, axis=1, bitorder="little"), F, 77, rng_mode=0, out=into) is into
+        assert np.array_equal(into, got)
     with pytest.raises(ValueError):
         s.sample_packed(np.zeros((3, 1), np.uint8), n_f + 9, 1)
+    with pytest.raises(ValueError):
+        s.sample_packed(np.zeros((3, (n_f + 7) // 8), np.uint8), n_f, 1, out=np.zeros((2, 1), np.uint8))
 
 
 def test_packed_io_without_f_columns(cuda_device):
