@@ -286,10 +286,10 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             // factor = 1 + (-1)^parity w^(phase & 3).  Every factor has
             // valuation <= 2 and the reference halves at most once per
             // factor, so the block's result is order-independent:
-            // prod / 2^floor(sum nu / 4).  Fast terms therefore run their
-            // columns grouped by rotation class (j = 0, 2, 1, 3), one
-            // branch-free loop per class; exact terms keep the reference's
-            // order.  The halving steps and the bound follow the run order.
+            // prod / 2^floor(sum nu / 4).  Fast terms therefore keep their
+            // columns grouped by rotation class (j = 0, 2, 1, 3) and reduce
+            // each class to a sign count (zring.cuh); exact terms keep the
+            // reference's order.
             struct NpCol { uint32_t phase; std::vector<uint64_t> m; };
             std::vector<NpCol> npc((size_t)cnp);
             for (int c = 0; c < cnp; ++c) {
