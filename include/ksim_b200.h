@@ -139,18 +139,21 @@ ksim_status ksim_component_sample_device(ksim_component *c, const uint8_t *d_f_s
  * in a latency-critical loop.  No reference counterpart: kokkos_sim always
  * allocates its Views inside Component.sample.
  *
- * The call allocates nothing.  Its scratch (the kernel's status word and the
- * staging chunk directory) is one fixed array of KSIM_NOALLOC_SCRATCH_BYTES in
- * device memory, loaded with the library on every GPU that uses it and held
- * until the process exits.  A component needing more than
- * KSIM_NOALLOC_MAX_CHUNKS staging chunks is rejected with
- * KSIM_ERR_UNSUPPORTED.  The first call on a device looks up the array's
- * device address; make that first call before any stream capture.  Every call
- * shares the array and leaves its contents behind (each call clears the status
- * word and rewrites the directory on `stream` before its kernel), so calls
- * that overlap on the GPU (other streams, other threads) race on it: issue
- * them on one stream. */
-#define KSIM_NOALLOC_SCRATCH_BYTES 33024
+ * The call allocates nothing.  Its scratch (the staging chunk directory) is
+ * one fixed array of KSIM_NOALLOC_SCRATCH_BYTES in device memory, loaded with
+ * the library on every GPU that uses it and held until the process exits.  A
+ * component needing more than KSIM_NOALLOC_MAX_CHUNKS staging chunks (or an
+ * image above 4 GiB) is rejected with KSIM_ERR_UNSUPPORTED.  The directory
+ * reaches the array as the by-value parameter of a one-CTA kernel queued on
+ * `stream` before the sampling kernel, so no host buffer is copied and the
+ * call does not wait for the stream.  The kernels' KSIM_FLAG_* bits (wait
+ * timeout, int64 risk, ...) go to the component's status word, read with
+ * ksim_component_status as for every other sampling call.  The first call on
+ * a device looks up the array's device address; make that first call before
+ * any stream capture.  Every call shares the array and leaves its directory
+ * behind, so calls that overlap on the GPU (other streams, other threads)
+ * race on it: issue them on one stream. */
+#define KSIM_NOALLOC_SCRATCH_BYTES 32768
 #define KSIM_NOALLOC_MAX_CHUNKS 1024
 ksim_status ksim_component_sample_device_noalloc(ksim_component *c, const uint8_t *d_f_sel,
                                                  int64_t B, int64_t shot_offset, uint64_t seed,
@@ -182,6 +185,17 @@ ksim_status ksim_component_set_launch(ksim_component *c, int32_t threads, int32_
                                       int32_t slot_bytes);
 ksim_status ksim_component_get_launch(const ksim_component *c, int32_t *threads, int32_t *staged,
                                       int32_t *slot_bytes);
+/* Bound of the staging waits of this component's sampling kernels (plain,
+ * batched, served and allocation-free), in non-blocking polls of the
+ * mbarrier 64 ns apart: a wait that runs out raises KSIM_FLAG_WAIT_TIMEOUT,
+ * the CTA waits (with the built-in bound) for the copies it issued and leaves
+ * without writing its shots, and the synchronous host calls report
+ * KSIM_ERR_TIMEOUT (and clear the flag they report).  0 restores the built-in
+ * bound (2^22 blocking try_wait polls).  Batches and server jobs take the
+ * value in force when they are created or admitted.  The reference has no bounded waits
+ * (kokkos_sim.cpp:188-241 fences without a limit); this is the failure
+ * detector's knob, and a small value lets a test see it fire. */
+ksim_status ksim_component_set_wait_limit(ksim_component *c, int64_t polls);
 /* Image statistics: terms, terms on the exact (overflow-risk) path, columns,
  * largest term record in bytes. */
 ksim_status ksim_component_stats(const ksim_component *c, int64_t *n_terms, int64_t *n_slow_terms,

@@ -205,6 +205,7 @@ def _declare(L: ctypes.CDLL) -> None:
         "ksim_component_eval_terms": (i32, [vp, i32, _u8p, i64, i64, i64p]),
         "ksim_component_status": (i32, [vp, ctypes.POINTER(u32), i32]),
         "ksim_component_set_launch": (i32, [vp, i32, i32, i32]),
+        "ksim_component_set_wait_limit": (i32, [vp, i64]),
         "ksim_component_get_launch": (i32, [vp, ctypes.POINTER(i32), ctypes.POINTER(i32),
                                             ctypes.POINTER(i32)]),
         "ksim_component_stats": (i32, [vp, i64p, i64p, i64p, i64p]),
@@ -257,19 +258,24 @@ class KsimError(RuntimeError):
         self.status = status
 
 
+def status_error(status: int, msg: str) -> Exception:
+    """The exception a non-OK ``ksim_status`` maps to (ValueError for bad
+    arguments, as the reference's std::invalid_argument surfaces)."""
+    if status in (KSIM_ERR_INVALID_ARGUMENT, KSIM_ERR_MALFORMED_PROGRAM):
+        return ValueError(msg)
+    if status == KSIM_ERR_OUT_OF_MEMORY:
+        return MemoryError(msg)
+    if status == KSIM_ERR_TIMEOUT:
+        return TimeoutError(msg)
+    return KsimError(status, msg)
+
+
 def check(status: int) -> None:
-    """Map a ``ksim_status`` to an exception (ValueError for bad arguments,
-    as the reference's std::invalid_argument surfaces)."""
+    """Raise the exception of a failing ``ksim_status`` with the library's
+    message of the last failing call on this thread."""
     if status == KSIM_OK:
         return
-    msg = (lib().ksim_last_error() or b"").decode(errors="replace")
-    if status in (KSIM_ERR_INVALID_ARGUMENT, KSIM_ERR_MALFORMED_PROGRAM):
-        raise ValueError(msg)
-    if status == KSIM_ERR_OUT_OF_MEMORY:
-        raise MemoryError(msg)
-    if status == KSIM_ERR_TIMEOUT:
-        raise TimeoutError(msg)
-    raise KsimError(status, msg)
+    raise status_error(status, (lib().ksim_last_error() or b"").decode(errors="replace"))
 
 
 def u8ptr(a: np.ndarray):

@@ -85,6 +85,21 @@ ksim_status component_chunks(ksim_component *c, int slot_bytes, const ChunkDir *
     return KSIM_OK;
 }
 
+// After a synchronous call: KSIM_ERR_TIMEOUT if a staging wait of the
+// component's kernels ran out, clearing that flag (the other flags stay for
+// ksim_component_status).
+ksim_status report_timeout(ksim_component *c)
+{
+    uint32_t flags = 0;
+    cudaError_t e = cudaMemcpy(&flags, c->d_status, sizeof(flags), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "status read");
+    if (!(flags & KSIM_FLAG_WAIT_TIMEOUT)) return KSIM_OK;
+    const uint32_t rest = flags & ~(uint32_t)KSIM_FLAG_WAIT_TIMEOUT;
+    e = cudaMemcpy(c->d_status, &rest, sizeof(rest), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "status write");
+    return fail(KSIM_ERR_TIMEOUT, "a staging wait of the sampling kernel ran out; its shots were not written");
+}
+
 // Fill a SampleJob for component c; inputs/outputs set by the caller.
 ksim_status component_job(ksim_component *c, const LaunchCfg &cfg, SampleJob &j)
 {
@@ -102,6 +117,7 @@ ksim_status component_job(ksim_component *c, const LaunchCfg &cfg, SampleJob &j)
     j.n_out = c->img.n_out;
     j.slot_bytes = slot;
     j.status = c->d_status;
+    j.wait_limit = c->wait_limit;
     return KSIM_OK;
 }
 
@@ -234,6 +250,15 @@ ksim_status ksim_component_set_launch(ksim_component *c, int32_t threads, int32_
     return KSIM_OK;
 }
 
+ksim_status ksim_component_set_wait_limit(ksim_component *c, int64_t polls)
+{
+    if (!c) return fail(KSIM_ERR_INVALID_ARGUMENT, "component is NULL");
+    if (polls < 0) return fail(KSIM_ERR_INVALID_ARGUMENT, "polls must be >= 0");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->wait_limit = polls;
+    return KSIM_OK;
+}
+
 ksim_status ksim_component_get_launch(const ksim_component *c, int32_t *threads, int32_t *staged,
                                       int32_t *slot_bytes)
 {
@@ -342,11 +367,7 @@ ksim_status ksim_component_sample(ksim_component *c, const uint8_t *f_sel, int64
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync(out)");
     e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cuda_fail(e, "sample");
-    uint32_t flags = 0;
-    e = cudaMemcpy(&flags, c->d_status, sizeof(flags), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return cuda_fail(e, "status read");
-    if (flags & KSIM_FLAG_WAIT_TIMEOUT) return fail(KSIM_ERR_TIMEOUT, "a staging wait timed out");
-    return KSIM_OK;
+    return report_timeout(c);
 }
 
 static ksim_status eval_common(ksim_component *c, int32_t graph, const uint8_t *params, int64_t B, int64_t P,
@@ -676,13 +697,12 @@ ksim_status program_sample_host(ksim_program *p, const uint8_t *f, int64_t B, in
     }
     if (st != KSIM_OK) return st;
     if (e != cudaSuccess) return cuda_fail(e, "program sample");
+    ksim_status rep = KSIM_OK;
     for (auto &part : p->parts) {
-        uint32_t flags = 0;
-        e = cudaMemcpy(&flags, part.comp->d_status, sizeof(flags), cudaMemcpyDeviceToHost);
-        if (e != cudaSuccess) return cuda_fail(e, "status read");
-        if (flags & KSIM_FLAG_WAIT_TIMEOUT) return fail(KSIM_ERR_TIMEOUT, "a staging wait timed out");
+        const ksim_status r = report_timeout(part.comp);
+        if (rep == KSIM_OK) rep = r;
     }
-    return KSIM_OK;
+    return rep;
 }
 
 }  // namespace

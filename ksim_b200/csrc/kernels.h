@@ -50,6 +50,8 @@ struct SampleJob {
     int64_t B, shot_offset;
     uint64_t seed;
     uint32_t *status;          // KSIM_FLAG_* accumulator
+    int64_t wait_limit;        // > 0: a staging wait gives up after this many test_wait polls
+    int64_t reserved;
 };
 
 struct LaunchCfg {

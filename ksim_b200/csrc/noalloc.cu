@@ -1,22 +1,27 @@
 // noalloc.cu — the sampler for callers that cannot allocate device memory.
 //
-// ksim_component_sample_device keeps its per-call working data (the status
-// word the kernel ORs its KSIM_FLAG_* bits into, and the chunk directory that
-// drives the shared-memory staging ring) in buffers the library allocates
-// with cudaMalloc on first use.  Some callers cannot allow that: code whose
-// device memory is owned by another allocator (a framework's caching pool, a
-// serving process that pre-reserves all of HBM), code that must not take the
-// implicit device synchronisation a cudaMalloc / cudaFree can cause inside a
-// latency-critical loop, or an embedding that forbids new allocations after
-// start-up.  ksim_component_sample_device_noalloc serves them: its scratch
-// is one file-scope __device__ array of fixed size, loaded with the library,
-// so the call itself allocates nothing.
+// ksim_component_sample_device keeps the chunk directory that drives the
+// shared-memory staging ring in a buffer the library allocates with
+// cudaMalloc on the first call for each staging slot size.  Some callers
+// cannot allow that: code whose device memory is owned by another allocator
+// (a framework's caching pool, a serving process that pre-reserves all of
+// HBM), code that must not take the implicit device synchronisation a
+// cudaMalloc / cudaFree can cause inside a latency-critical loop, or an
+// embedding that forbids new allocations after start-up.
+// ksim_component_sample_device_noalloc serves them: its scratch is one
+// file-scope __device__ array of fixed size, loaded with the library, so the
+// call itself allocates nothing.
 //
-// Scratch layout: [status word, padded to 256 B][chunk directory].  The
-// array holds at most NOALLOC_MAX_CHUNKS chunk records; components that need
-// more are rejected with KSIM_ERR_UNSUPPORTED.  Every call shares the array:
-// each call clears the status word and rewrites the directory on its stream,
-// so calls on one stream follow each other correctly, while calls that
+// The scratch holds the chunk directory, at most NOALLOC_MAX_CHUNKS records;
+// components that need more are rejected with KSIM_ERR_UNSUPPORTED.  Each
+// call builds the directory on the host (on the stack) and hands it to a
+// one-CTA kernel as a by-value kernel parameter; that kernel writes it into
+// the array and the sampling kernel follows on the same stream.  No host
+// buffer is copied, so the call never waits for the stream.  The kernels'
+// KSIM_FLAG_* bits go to the component's own status word (allocated when the
+// component was created), read with ksim_component_status like those of every
+// other sampling call.  Every call shares the array and leaves its directory
+// behind: calls on one stream follow each other correctly, while calls that
 // overlap on the GPU (different streams, or different host threads) race on
 // it and must not be issued.
 #include <cuda_runtime.h>
@@ -33,9 +38,8 @@
 namespace ksim {
 namespace {
 
-constexpr int NOALLOC_DIR_OFFSET = 256;
 constexpr int NOALLOC_MAX_CHUNKS = 1024;
-constexpr size_t NOALLOC_SCRATCH_BYTES = NOALLOC_DIR_OFFSET + NOALLOC_MAX_CHUNKS * sizeof(ChunkDir);
+constexpr size_t NOALLOC_SCRATCH_BYTES = NOALLOC_MAX_CHUNKS * sizeof(ChunkDir);
 constexpr int NOALLOC_MAX_DEVICES = 64;
 
 static_assert(KSIM_NOALLOC_SCRATCH_BYTES == NOALLOC_SCRATCH_BYTES, "header and scratch size disagree");
@@ -48,6 +52,31 @@ __device__ __align__(256) uint8_t g_sample_scratch[NOALLOC_SCRATCH_BYTES];
 // symbol itself: on the host it names a stand-in, not device memory).
 std::mutex g_scratch_mu;
 uint8_t *g_scratch_addr[NOALLOC_MAX_DEVICES] = {};
+
+// The chunk directory as a kernel parameter: 16 bytes per chunk (term-stream
+// offset, bytes, graph, term count with the end-of-graph flag in bit 31).
+struct DirParam {
+    int32_t n, pad[3];
+    uint4 rec[NOALLOC_MAX_CHUNKS];
+};
+static_assert(sizeof(DirParam) <= 32764, "kernel parameters are limited to 32,764 bytes");
+
+__global__ void __launch_bounds__(256) k_noalloc_dir(const __grid_constant__ DirParam d)
+{
+    ChunkDir *out = (ChunkDir *)g_sample_scratch;
+    for (int i = threadIdx.x; i < d.n; i += blockDim.x) {
+        const uint4 r = d.rec[i];
+        ChunkDir c;
+        c.off = (int64_t)r.x;
+        c.bytes = (int32_t)r.y;
+        c.graph = (int32_t)r.z;
+        c.n_terms = (int32_t)(r.w & 0x7FFFFFFFu);
+        c.end_of_graph = (int32_t)(r.w >> 31);
+        c.pad0 = 0;
+        c.pad1 = 0;
+        out[i] = c;
+    }
+}
 
 template <int W, bool STAGED>
 __global__ void __launch_bounds__(256, KSIM_SAMPLE_MIN_CTAS) k_sample_noalloc(const SampleJob j)
@@ -79,10 +108,10 @@ ksim_status scratch_address(int dev, uint8_t **out)
     return KSIM_OK;
 }
 
-// The chunk directory of `img` for a staging slot, written into a fixed
-// array: returns the count, -1 if a term exceeds the slot, -2 if more than
-// `cap` chunks are needed.  Same chunking rule as make_chunks (image.cpp).
-int chunks_into(const HostImage &img, int64_t slot_bytes, ChunkDir *out, int cap)
+// The chunk directory of `img` for a staging slot, packed into `out`: returns
+// the count, -1 if a term exceeds the slot, -2 if more than `cap` chunks are
+// needed.  Same chunking rule as make_chunks (image.cpp).
+int chunks_into(const HostImage &img, int64_t slot_bytes, uint4 *out, int cap)
 {
     int n = 0;
     for (int k = 0; k < img.n_graphs; ++k) {
@@ -90,25 +119,17 @@ int chunks_into(const HostImage &img, int64_t slot_bytes, ChunkDir *out, int cap
         const int G = (int)to.size() - 1;
         if (G <= 0) {
             if (n == cap) return -2;
-            ChunkDir c = {};
-            c.off = img.gdir[k].stream_off;
-            c.graph = k;
-            c.end_of_graph = 1;
-            out[n++] = c;
+            out[n++] = make_uint4((uint32_t)img.gdir[k].stream_off, 0u, (uint32_t)k, 0x80000000u);
             continue;
         }
         for (int t = 0; t < G;) {
-            ChunkDir c = {};
-            c.off = to[t];
-            c.graph = k;
+            const int64_t off = to[t];
             int u = t;
-            while (u < G && to[u + 1] - c.off <= slot_bytes) ++u;
+            while (u < G && to[u + 1] - off <= slot_bytes) ++u;
             if (u == t) return -1;
             if (n == cap) return -2;
-            c.bytes = (int32_t)(to[u] - c.off);
-            c.n_terms = u - t;
-            c.end_of_graph = (u == G) ? 1 : 0;
-            out[n++] = c;
+            out[n++] = make_uint4((uint32_t)off, (uint32_t)(to[u] - off), (uint32_t)k,
+                                  (uint32_t)(u - t) | (u == G ? 0x80000000u : 0u));
             t = u;
         }
     }
@@ -172,18 +193,23 @@ extern "C" ksim_status ksim_component_sample_device_noalloc(ksim_component *c, c
         return fail(KSIM_ERR_INVALID_ARGUMENT, "input or output pointer is NULL");
     if (out_col0 < 0 || out_stride < out_col0 + c->img.n_out)
         return fail(KSIM_ERR_INVALID_ARGUMENT, "out_stride must be >= out_col0 + n_out");
+    if (c->image_bytes > 0xFFFFFFFFull)
+        return fail(KSIM_ERR_UNSUPPORTED, "program images above 4 GiB are beyond the fixed scratch's directory "
+                                          "records; use ksim_component_sample_device");
     DeviceGuard g(c->device);
     if (!g.ok) return fail(KSIM_ERR_CUDA, "cannot select the component's device");
     LaunchCfg cfg;
+    int64_t wait_limit;
     {
         std::lock_guard<std::mutex> lk(c->mu);
         cfg = c->cfg;
+        wait_limit = c->wait_limit;
     }
-    // the directory is built on the stack (no heap either) and copied into
-    // the scratch on the caller's stream
-    ChunkDir dir[NOALLOC_MAX_CHUNKS];
+    // the directory is built on the stack (no heap either) and travels as the
+    // parameter of the kernel that writes it into the scratch
+    DirParam dir;
     const int64_t chunk_slot = cfg.staged ? cfg.slot_bytes : (int64_t)1 << 30;
-    const int n = chunks_into(c->img, chunk_slot, dir, NOALLOC_MAX_CHUNKS);
+    const int n = chunks_into(c->img, chunk_slot, dir.rec, NOALLOC_MAX_CHUNKS);
     if (n == -1)
         return fail(KSIM_ERR_INVALID_ARGUMENT, "a term record is larger than the staging slot");
     if (n == -2)
@@ -191,19 +217,20 @@ extern "C" ksim_status ksim_component_sample_device_noalloc(ksim_component *c, c
                                               " staging chunks, the most the fixed scratch of "
                                               "ksim_component_sample_device_noalloc holds; use "
                                               "ksim_component_sample_device or a larger slot_bytes");
+    dir.n = n;
+    dir.pad[0] = dir.pad[1] = dir.pad[2] = 0;
     uint8_t *scratch = nullptr;
     ksim_status s = scratch_address(c->device, &scratch);
     if (s != KSIM_OK) return s;
     cudaStream_t st = (cudaStream_t)stream;
-    cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(uint32_t), st);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(scratch status)");
-    e = cudaMemcpyAsync(scratch + NOALLOC_DIR_OFFSET, dir, sizeof(ChunkDir) * (size_t)n, cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync(scratch chunk directory)");
+    k_noalloc_dir<<<1, 256, 0, st>>>(dir);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "chunk directory kernel launch (no-alloc)");
 
     SampleJob j = {};
     j.image = c->d_image;
     j.gdir = (const GraphDir *)c->d_image;
-    j.cdir = (const ChunkDir *)(scratch + NOALLOC_DIR_OFFSET);
+    j.cdir = (const ChunkDir *)scratch;
     j.n_chunks = n;
     j.n_graphs = c->img.n_graphs;
     j.F = c->img.F;
@@ -221,7 +248,8 @@ extern "C" ksim_status ksim_component_sample_device_noalloc(ksim_component *c, c
     j.B = B;
     j.shot_offset = shot_offset;
     j.seed = seed;
-    j.status = (uint32_t *)scratch;
+    j.status = c->d_status;
+    j.wait_limit = wait_limit;
     e = launch_noalloc(j, c->img.W, cfg, st);
     if (e != cudaSuccess) return cuda_fail(e, "sample kernel launch (no-alloc)");
     return KSIM_OK;

@@ -50,6 +50,7 @@ struct ksim_component {
     cudaStream_t stream = nullptr;
     ksim::DevBuf ws_f, ws_out, ws_aux;
     ksim::LaunchCfg cfg;
+    int64_t wait_limit = 0;  // polls of a staging wait (0: the kernels' default)
     std::mutex mu;        // workspaces and cfg
     std::mutex chunk_mu;  // the chunk-directory map
 };

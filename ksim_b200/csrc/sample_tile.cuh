@@ -40,6 +40,11 @@ namespace ksim {
 constexpr int NSLOT = 2;
 constexpr int BAR_BYTES = 128;
 static_assert(ROW_WORDS == NB_MAX + 1, "row-parity words per shot: one term's blocks and a spare");
+// Polls of an mbarrier wait before it gives up (each poll is one try_wait,
+// which itself suspends for a hardware-defined interval).  A job may set its
+// own bound (SampleJob::wait_limit) for the waits of its chunks, counted in
+// non-blocking test_wait polls 64 ns apart; the waits that drain a CTA's
+// copies after a timeout always use this one.
 constexpr long long WAIT_LIMIT = 1ll << 22;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -70,10 +75,10 @@ __device__ __forceinline__ void tma_bulk_g2s(void *dst, const void *src, uint32_
                  : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit = WAIT_LIMIT)
 {
     const uint32_t a = smem_u32(bar);
-    for (long long it = 0; it < WAIT_LIMIT; ++it) {
+    for (long long it = 0; it < limit; ++it) {
         uint32_t ok;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -83,6 +88,25 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
             : "r"(a), "r"(parity)
             : "memory");
         if (ok) return true;
+    }
+    return false;
+}
+
+// A wait of at most `polls` non-blocking tests, 64 ns apart (a job's own bound).
+__device__ __forceinline__ bool mbar_poll(uint64_t *bar, uint32_t parity, long long polls)
+{
+    const uint32_t a = smem_u32(bar);
+    for (long long it = 0; it < polls; ++it) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        __nanosleep(64);
     }
     return false;
 }
@@ -406,7 +430,8 @@ __device__ __forceinline__ bool sample_tile(const SampleJob &j, const int64_t s0
         const uint8_t *p;
         if (STAGED) {
             const int slot = (int)(gc & (NSLOT - 1));
-            const bool ok = mbar_wait(&bar[slot], (gc / NSLOT) & 1u);
+            const bool ok = j.wait_limit > 0 ? mbar_poll(&bar[slot], (gc / NSLOT) & 1u, j.wait_limit)
+                                             : mbar_wait(&bar[slot], (gc / NSLOT) & 1u);
             if (__syncthreads_or(!ok)) {
                 if (tid == 0) {
                     atomicOr(j.status, (uint32_t)KSIM_FLAG_WAIT_TIMEOUT);

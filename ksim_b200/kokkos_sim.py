@@ -141,6 +141,12 @@ class Component:
     def set_launch(self, threads: int = 0, staged: int = -1, slot_bytes: int = 0) -> None:
         check(self._L.ksim_component_set_launch(self._h, int(threads), int(staged), int(slot_bytes)))
 
+    def set_wait_limit(self, polls: int = 0) -> None:
+        """Bound of the staging waits of this component's kernels in mbarrier
+        polls (0: the built-in bound).  A wait that runs out makes the host
+        calls raise TimeoutError (KSIM_ERR_TIMEOUT)."""
+        check(self._L.ksim_component_set_wait_limit(self._h, int(polls)))
+
     def get_launch(self) -> dict:
         t, s, b = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
         check(self._L.ksim_component_get_launch(self._h, ctypes.byref(t), ctypes.byref(s),

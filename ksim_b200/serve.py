@@ -163,6 +163,8 @@ class Request:
             lat, t = ctypes.c_double(), ctypes.c_double()
             ms = -1 if timeout is None else max(0, int(timeout * 1000))
             st = L.ksim_server_wait(h, self.id, ms, ctypes.byref(lat), ctypes.byref(t))
+            # the request's own message, before another call replaces it
+            msg = (L.ksim_last_error() or b"").decode(errors="replace") if st else ""
             if st == _abi.KSIM_ERR_TIMEOUT:
                 flag = ctypes.c_int32()
                 if L.ksim_server_poll(h, self.id, ctypes.byref(flag)) == _abi.KSIM_OK:
@@ -171,10 +173,7 @@ class Request:
             self._done = True
             self._srv._retire(self.id)
             if st != _abi.KSIM_OK:
-                try:
-                    check(st)
-                except Exception as e:  # noqa: BLE001 - kept for re-raising
-                    self._error = e
+                self._error = _abi.status_error(st, msg)
             else:
                 self.latency_s, self.done_time_s = lat.value, t.value
         if self._error is not None:

@@ -35,6 +35,24 @@ def oracle_port():
     return oracle
 
 
+@pytest.fixture(scope="session")
+def oracle_module(oracle_port):
+    """The oracle module (``program_sample`` and the oracle classes)."""
+    return oracle_port
+
+
+@pytest.fixture(scope="session")
+def ref_oracle(oracle_port):
+    """The reference's own zx_eval.hpp (``oracle/_ref``) as an oracle class;
+    the C restatement (pinned to it bit for bit by the CPU suite) where that
+    library was not built."""
+    if oracle_port.RefOracle.available():
+        return oracle_port.RefOracle
+    import warnings
+    warnings.warn("oracle/_ref is not built: checking against the C restatement")
+    return oracle_port.PortOracle
+
+
 def _build_hostemu():
     srcs = [HOSTEMU_SRC, ROOT / "ksim_b200" / "csrc" / "image.cpp"]
     deps = srcs + list((ROOT / "ksim_b200" / "csrc").glob("*.cuh")) + \

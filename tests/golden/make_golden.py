@@ -13,11 +13,13 @@ per-term numerators canonicalised (divided by 2 while all four coefficients
 are even), ``zx_eval.hpp`` amplitudes (bit-exact reference), and
 ``zx_eval.hpp`` samples (bits and |A_k|) for two seeds in both uniform modes.
 
-Usage: python tests/golden/make_golden.py [--ref /root/reference]
+Usage: python tests/golden/make_golden.py [--ref <reference checkout>]
+(default: the KSIM_REF_TREE environment variable)
 """
 from __future__ import annotations
 
 import argparse
+import os
 import zlib
 import sys
 import types
@@ -132,8 +134,11 @@ def fixture_programs():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("KSIM_REF_TREE"),
+                    help="root of the reference checkout (default: $KSIM_REF_TREE)")
     a = ap.parse_args()
+    if not a.ref:
+        raise SystemExit("give --ref or set KSIM_REF_TREE to the reference checkout")
     ref = Path(a.ref)
     evaluate, es = import_reference_numpy(ref)
     from oracle.oracle import RefOracle, build

@@ -9,11 +9,13 @@ each parity computed from the reference's precomputed sparse channel data
 (``_precompute_sparse``, after its channel simplification), and the parity
 frequencies of 200,000 shots drawn by the reference's ``sample``.
 
-Usage: python tests/golden/make_noise_golden.py [--ref /root/reference]
+Usage: python tests/golden/make_noise_golden.py [--ref <reference checkout>]
+(default: the KSIM_REF_TREE environment variable)
 """
 from __future__ import annotations
 
 import argparse
+import os
 import importlib.util
 import sys
 from pathlib import Path
@@ -62,8 +64,11 @@ def exact_from_sparse(sparse, cols):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("KSIM_REF_TREE"),
+                    help="root of the reference checkout (default: $KSIM_REF_TREE)")
     a = ap.parse_args()
+    if not a.ref:
+        raise SystemExit("give --ref or set KSIM_REF_TREE to the reference checkout")
     ch = load_channels(Path(a.ref))
     rng = np.random.default_rng(20261203)
     for name, (probs, T) in models(ch, rng).items():
