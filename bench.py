@@ -15,19 +15,28 @@ JSON line on rank 0.
 * ``e2e``: the same metric through the public drop-in API
   (``B200ProgramSampler.sample``) from pinned host memory, host<->device
   copies inside the timed region.
-* ``roofline``: integer-ALU bound; algorithmic int32 ops per launch
-  (ksim_b200.perfmodel) / event time vs the integer-pipe peak measured on
-  this GPU by ksim_measure_int_peak.
+* ``roofline``: instruction-issue bound: thread instructions per shot (one
+  ncu capture, NCU_THREAD_INST_PER_SHOT) x shots/s over SMs x 4 issue slots
+  x 32 lanes x the sampled SM clock; beside it both int32 op models (the
+  formulation's and the reference algorithm's) against two measured integer
+  peaks (the sampler's add/shift/logic mix and add/logic alone).
+* ``parity``: the first rows of the last timed output and of the last e2e
+  output against the reference's own zx_eval.hpp (oracle/_ref).
 * ``cpu_baseline``: the reference's own zx_eval.hpp (oracle/_ref) or its C
-  restatement, all host threads, on a bounded shot sample.
+  restatement, all host threads, on a bounded shot sample;
+  ``cpu_baseline_numpy``: the reference's numpy sample_flat (restated in
+  oracle/numpy_flat.py), one process, on a bounded prefix.
+* ``legs``: cfg1 (5 outputs, t = 4, 1e5 shots) and cfg4 (16 parity outputs,
+  t = 20, 1e6 shots) through the same plain path, with e2e and parity.
 * ``batched`` (1 GPU): 64 seeded programs (qubits U[8,60], t U[2,16], shots
   log-uniform 1e3-1e5) in one persistent graph-replayed launch, autotuned,
   vs 64 plain one-program launches; device time, L2 flushed, bit identity
   of the two checked.
 * ``served`` (1 GPU): 10 000 Poisson requests over a 200-program pool at
-  80 % of the measured served capacity through the continuous-batching
-  server: shots/s and p50/p99 latency (arrival -> bits in host memory, host
-  clock), vs the same stream through plain per-request calls.
+  80 % of the batched capacity of the same request mix (its first requests
+  run as one autotuned batch) through the continuous-batching server:
+  shots/s and p50/p99 latency (arrival -> bits in host memory, host clock),
+  vs the same stream through plain per-request calls.
 
 ``--impl reference`` times that CPU implementation alone on the same workload
 (rank 0 only under torchrun).
@@ -57,6 +66,11 @@ L2_FLUSH_BYTES = 256 << 20
 # dram__bytes_write.sum), plus the output row the capture's L2 absorbed;
 # scaled to a launch by its shots.  Source: profiles/k_sample_cfg2_current.md.
 NCU_DRAM_BYTES_PER_SHOT = {"cfg2-medium-40q-t12": 66.2 + 40.0}
+# Thread instructions per shot of the plain kernel on the same workload, from
+# one ncu capture (smsp__thread_inst_executed.sum / shots of the captured
+# launch); the issue roofline of the bench line is this times shots/s over
+# the SMs' issue ceiling.  Source: profiles/k_sample_cfg2_current.md.
+NCU_THREAD_INST_PER_SHOT = {}
 
 
 def parse():
@@ -74,7 +88,16 @@ def parse():
     ap.add_argument("--no-served", action="store_true", help="skip the served (request stream) leg")
     ap.add_argument("--requests", type=int, default=10_000, help="requests of the served leg")
     ap.add_argument("--load", type=float, default=0.8,
-                    help="served arrival rate as a fraction of the measured served capacity")
+                    help="served arrival rate as a fraction of the batched capacity measured "
+                         "on the request mix")
+    ap.add_argument("--legs", default="1,4",
+                    help="extra plain workloads timed beside the headline one (config numbers)")
+    ap.add_argument("--parity-shots", type=int, default=4096,
+                    help="shots of each timed output checked against the reference oracle")
+    ap.add_argument("--numpy-seconds", type=float, default=8.0,
+                    help="CPU seconds of the numpy sample_flat baseline")
+    ap.add_argument("--serve-threads", type=int, default=0,
+                    help="threads per CTA of the serving loop (0: the library default)")
     return ap.parse_args()
 
 
@@ -207,6 +230,51 @@ def cpu_reference_rate(prog, f, seed, rng_mode, target_s, max_shots):
     return n2 / dt, kind, threads, n2, dt
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (for the CPU-baseline records)."""
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.lower().startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def parity_check(prog, f_rows, bits, seed, rng_mode, shot_offset=0):
+    """Compare sampled rows with the reference's own zx_eval.hpp (oracle/_ref,
+    or its C restatement where that is not built), all host threads."""
+    from oracle import oracle as orc
+    if not orc.PORT_LIB.exists():
+        orc.build()
+    cls = orc.RefOracle if orc.RefOracle.available() else orc.PortOracle
+    want = orc.program_sample(prog, f_rows, seed, rng_mode, oracle_cls=cls, shot_offset=shot_offset)
+    return {"shots": int(f_rows.shape[0]), "ok": bool(np.array_equal(bits, want)),
+            "checker": "oracle/_ref (zx_eval.hpp)" if cls is orc.RefOracle else "C restatement"}
+
+
+def numpy_baseline(prog, f, target_s):
+    """Shots/s of the reference's numpy sample_flat (restated in
+    oracle/numpy_flat.py, one process) on a prefix sized to ~target_s."""
+    from oracle import numpy_flat as nf
+    import warnings
+    n = min(32, f.shape[0])
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        t0 = time.perf_counter()
+        nf.sample_flat(prog, f[:n], np.random.default_rng(1))
+        dt = time.perf_counter() - t0
+        n2 = int(min(f.shape[0], max(n, n * target_s / max(dt, 1e-6))))
+        t0 = time.perf_counter()
+        nf.sample_flat(prog, f[:n2], np.random.default_rng(2))
+        dt = time.perf_counter() - t0
+    return {"value": n2 / dt, "unit": "shots/s", "cores": 1, "kind": "port",
+            "cpu_model": cpu_model(),
+            "sample": f"first {n2} shots, {dt:.1f} s: numpy sample_flat (evaluate.py:69-87) "
+                      f"restated in oracle/numpy_flat.py, bit-identical to the reference's"}
+
+
 def arm_config(w, shots, n_f, rng, world):
     """The config object both arms print (same workload, same keys)."""
     n_out = int(len(w.program.output_order))
@@ -255,7 +323,7 @@ def run_reference(args):
             "config": arm_config(w, shots, f.shape[1], args.rng, args.gpus),
             "step_shots": step_shots,
             "cpu_baseline": {"value": value, "unit": "shots/s", "cores": threads, "kind": kind,
-                             "sample": sample},
+                             "cpu_model": cpu_model(), "sample": sample},
             "e2e": {"value": value, "unit": "shots/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -272,6 +340,55 @@ def _timed_launches(torch, stream, flush, fn, steps):
         evs[i][1].record(stream)
     torch.cuda.synchronize()
     return [a.elapsed_time(b) for a, b in evs]
+
+
+def plain_leg(args, torch, dev, flush, cfg):
+    """Another single-program workload through the plain path: device-timed
+    shots/s (inputs resident, L2 flushed), the drop-in call from pinned host
+    buffers, and the first rows of both outputs against the reference oracle."""
+    from ksim_b200 import _abi, perfmodel, synth
+    from ksim_b200.sampler import B200ProgramSampler
+    L = _abi.lib()
+    w = synth.config(cfg)
+    shots = w.shots
+    f = synth.sample_f(np.random.default_rng(w.seed + 1), shots, w.n_f, w.f_prob)
+    s = B200ProgramSampler(w.program, device=dev.index or 0)
+    n_out = s.num_outputs
+    d_f = torch.from_numpy(f).to(dev)
+    d_out = torch.zeros((shots, n_out), dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def launch(seed):
+        _abi.check(L.ksim_program_sample_device(
+            s.handle, ctypes.c_void_p(d_f.data_ptr()), shots, w.n_f, 0, seed, args.rng,
+            ctypes.c_void_p(d_out.data_ptr()), ctypes.c_void_p(stream.cuda_stream)))
+
+    for i in range(max(3, args.warmup)):
+        launch(100 + i)
+    steps = max(3, args.steps)
+    ts = _timed_launches(torch, stream, flush, lambda i: launch(200 + i), steps)
+    ms = sum(ts) / len(ts)
+    n_chk = min(shots, args.parity_shots if cfg != 1 else shots)
+    dev_par = parity_check(w.program, f[:n_chk], d_out[:n_chk].cpu().numpy(), 200 + steps - 1, args.rng)
+    f_pin = torch.from_numpy(f).pin_memory().numpy()
+    out_pin = torch.empty((shots, n_out), dtype=torch.uint8).pin_memory().numpy()
+    s.sample(f_pin, 300, rng_mode=args.rng, out=out_pin)
+    e2e = []
+    for i in range(steps):
+        t0 = time.perf_counter()
+        s.sample(f_pin, 400 + i, rng_mode=args.rng, out=out_pin)
+        e2e.append(time.perf_counter() - t0)
+    e2e_par = parity_check(w.program, f[:n_chk], out_pin[:n_chk], 400 + steps - 1, args.rng)
+    work = perfmodel.program_work(w.program)
+    return {"workload": arm_config(w, shots, w.n_f, args.rng, 1)["workload"], "shots": shots,
+            "value": shots / (ms / 1e3), "unit": "shots/s", "ms_per_step": ms, "steps": steps,
+            "e2e": {"value": shots * steps / sum(e2e), "unit": "shots/s",
+                    "h2d_bytes_per_step": int(f.nbytes), "d2h_bytes_per_step": int(shots * n_out),
+                    "api": "B200ProgramSampler.sample (ksim_program_sample), pinned buffers"},
+            "ops_per_shot": work["ops"],
+            "ops_per_shot_reference_model": perfmodel.reference_op_model(w.program),
+            "parity": {"device_output": dev_par, "e2e_output": e2e_par},
+            "gpu_launches": steps * len(w.program.components)}
 
 
 def bench_batched(args, torch, dev, flush):
@@ -376,6 +493,26 @@ def _replay(arrivals, submit, collect):
     return t0, done
 
 
+def _batched_capacity(torch, dev, pool, pidx, shots, wide, r0, seeds, rng_mode):
+    """Shots/s of requests (pool[pidx[i]], shots[i] rows of `wide` from r0[i],
+    seeds[i]) run as one autotuned BatchSampler launch."""
+    from ksim_b200.batch import BatchSampler
+    progs = [pool[int(p)].program for p in pidx]
+    nfs = [pool[int(p)].n_f for p in pidx]
+    bs = BatchSampler(progs, [int(b) for b in shots], seeds=[int(s) for s in seeds], rng_mode=rng_mode,
+                      device=dev.index or 0, n_f=nfs)
+    bs.set_inputs([wide[int(a):int(a) + int(b), :nf] for a, b, nf in zip(r0, shots, nfs)])
+    rec = bs.tune()
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(3):
+        bs.launch(stream)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    ts = _timed_launches(torch, stream, flush, lambda i: bs.launch(stream), 5)
+    cap = float(np.sum(shots)) / (sum(ts) / len(ts) / 1e3)
+    del bs
+    return cap, rec["tuning"]
+
+
 def bench_served(args, torch, dev):
     """Workload 5: a Poisson stream of sample requests over a 200-program pool
     through the continuous-batching server, and the same stream through plain
@@ -395,7 +532,7 @@ def bench_served(args, torch, dev):
     n_out = [p.program.num_outputs for p in pool]
     ring = _PinnedRing(torch, 1 << 30)
 
-    srv = Server(device=dev.index or 0, arena_bytes=4 << 30)
+    srv = Server(device=dev.index or 0, arena_bytes=4 << 30, threads=args.serve_threads)
     for w in pool:                       # programs resident on the device before the stream
         d, _ = srv.cache.acquire(w.program)
         srv.cache.release(d)
@@ -411,11 +548,15 @@ def bench_served(args, torch, dev):
         ring.free_oldest()
         return h.done_time_s
 
-    # capacity: a closed burst of the first requests, all submitted at once
+    # batched capacity of this request mix: the first requests as one
+    # persistent, autotuned, graph-replayed batch (inputs resident, device time)
     n_probe = min(n_req, 1500)
+    batched_capacity, batched_tuning = _batched_capacity(torch, dev, pool, pidx[:n_probe], shots[:n_probe],
+                                                         wide, r0[:n_probe], seeds[:n_probe], args.rng)
+    # served capacity: a closed burst of the same requests, all submitted at once
     t0, done = _replay([0.0] * n_probe, submit, collect)
     capacity = float(shots[:n_probe].sum()) / (max(done) - t0)
-    rate = args.load * capacity / float(shots.mean())
+    rate = args.load * batched_capacity / float(shots.mean())
     arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
     before = srv.stats()
     t0, done = _replay(arrivals, submit, collect)
@@ -442,7 +583,10 @@ def bench_served(args, torch, dev):
             "shots_per_s": served, "p50_ms": q(lat, 50), "p99_ms": q(lat, 99),
             "plain_shots_per_s": plain, "plain_p50_ms": q(plat, 50), "plain_p99_ms": q(plat, 99),
             "speedup_vs_plain": served / plain,
-            "arrival_rate_per_s": rate, "load": args.load, "capacity_shots_per_s": capacity,
+            "arrival_rate_per_s": rate, "load": args.load,
+            "load_basis": "batched capacity of the request mix (first requests as one batch)",
+            "batched_capacity_shots_per_s": batched_capacity, "batched_tuning": batched_tuning,
+            "served_capacity_shots_per_s": capacity,
             "total_shots": int(shots.sum()),
             "loop_launches": st["loop_launches"] - before["loop_launches"],
             "failed": st["failed"], "clock": "host wall clock, arrival -> results in host memory"}
@@ -481,6 +625,8 @@ def main():
 
     peak = ctypes.c_double()
     _abi.check(L.ksim_measure_int_peak(local, ctypes.byref(peak), None))
+    alu_peak = ctypes.c_double()
+    _abi.check(L.ksim_measure_alu_peak(local, ctypes.byref(alu_peak), None))
 
     for i in range(args.warmup):
         launch(1000 + i)
@@ -504,6 +650,12 @@ def main():
     total_ms = max_over_ranks(sum(step_ms), world)
     value = world * shots * args.steps / (total_ms / 1e3)
     ms_per_step = total_ms / args.steps
+    parity = {}
+    if rank == 0:
+        # the last timed launch's first rows against the reference oracle
+        n_chk = min(shots, args.parity_shots)
+        parity["device_output"] = parity_check(prog, f[:n_chk], d_out[:n_chk].cpu().numpy(),
+                                               2000 + args.steps - 1, args.rng, shot_offset=offset)
 
     # end to end through the drop-in API, pinned host buffers in and out
     f_pin = torch.from_numpy(f).pin_memory().numpy()
@@ -518,6 +670,10 @@ def main():
         e2e_t.append(time.perf_counter() - t0)
     e2e_total = max_over_ranks(sum(e2e_t), world)
     e2e_value = world * shots * args.steps / e2e_total
+    if rank == 0:
+        n_chk = min(shots, args.parity_shots)
+        parity["e2e_output"] = parity_check(prog, f[:n_chk], out_pin[:n_chk], 4000 + args.steps - 1,
+                                            args.rng)
     # the same through the bit-packed entry point (8 f columns / outputs per byte)
     fp_pin = torch.from_numpy(np.packbits(f, axis=1, bitorder="little")).pin_memory().numpy()
     op_pin = torch.empty((shots, (n_out + 7) // 8), dtype=torch.uint8).pin_memory().numpy()
@@ -551,8 +707,18 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, kind, cores, n, dt = cpu_reference_rate(prog, f, 2000, args.rng, args.cpu_seconds,
                                                       shots)
-        cpu = {"value": rate, "unit": "shots/s", "cores": cores, "kind": kind,
-               "sample": f"first {n} shots of {w.name}, {dt:.1f} s on {cores} threads"}
+        cpu = {"value": rate, "unit": "shots/s", "cores": cores, "kind": kind, "cpu_model": cpu_model(),
+               "sample": f"first {n} shots of {w.name}, {dt:.1f} s on {cores} threads "
+                         "(zx_eval.hpp + restated kokkos_sim loop, OpenMP)"}
+    cpu_numpy = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu_numpy = numpy_baseline(prog, f, args.numpy_seconds)
+
+    legs = {}
+    if world == 1:
+        for c in [int(x) for x in args.legs.split(",") if x.strip()]:
+            if c != args.workload:
+                legs[f"cfg{c}"] = plain_leg(args, torch, dev, flush, c)
 
     batched = served = None
     if world == 1 and not args.no_batched:
@@ -564,6 +730,43 @@ def main():
         mean_s = (sum(step_ms) / len(step_ms)) / 1e3
         achieved = work["ops"] * shots / mean_s
         hbm_bytes = shots * (work["in_bytes"] + work["out_bytes"])
+        clocks = clk.summary()
+        sm_mhz = clocks["sm_mhz"] or clocks["sm_max_mhz"] or 1965.0
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        # issue ceiling: every SM sub-partition issues one warp instruction a clock
+        issue_peak = sms * 4 * 32 * sm_mhz * 1e6
+        inst = NCU_THREAD_INST_PER_SHOT.get(w.name)
+        issue = inst * shots / mean_s if inst else None
+        ref_ops = perfmodel.reference_op_model(prog)
+        roofline = {
+            "bound": "issue",
+            "achieved": issue / 1e12 if issue else None,
+            "peak": issue_peak / 1e12,
+            "unit": "T thread-instructions/s",
+            "frac": issue / issue_peak if issue else None,
+            "issue_frac": issue / issue_peak if issue else None,
+            "inst_per_shot": inst,
+            "inst_source": "ncu smsp__thread_inst_executed.sum of k_sample on this workload / shots "
+                           "(profiles/k_sample_cfg2_current.md)",
+            "peak_source": f"{sms} SMs x 4 issue slots x 32 lanes x median sampled SM clock "
+                           f"({sm_mhz:.0f} MHz)",
+            "ops_per_shot": work["ops"],
+            "ops_per_shot_reference_model": ref_ops,
+            "ops_note": "ops_per_shot: int32 operations of the formulation the kernels run; "
+                        "ops_per_shot_reference_model: the reference's step-by-step algorithm "
+                        "(84 per Z[w] product, 5 per 64-bit parity word); neither is an issue count",
+            "int_ops_per_s": achieved,
+            "int_peak_mixed": peak.value,
+            "int_peak_alu": alu_peak.value,
+            "ops_frac_of_mixed_peak": achieved / peak.value,
+            "ops_frac_of_alu_peak": achieved / alu_peak.value,
+            "reference_model_ops_per_s": ref_ops * shots / mean_s,
+            "traffic": (NCU_DRAM_BYTES_PER_SHOT[w.name] * shots
+                        if w.name in NCU_DRAM_BYTES_PER_SHOT else None),
+            "traffic_unit": "bytes per launch",
+            "algorithmic_bytes": hbm_bytes,
+            "hbm_gbs": hbm_bytes / mean_s / 1e9,
+        }
         line = {
             "metric": METRIC, "value": value, "unit": "shots/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -581,18 +784,14 @@ def main():
                            "h2d_bytes_per_step": int(fp_pin.nbytes),
                            "d2h_bytes_per_step": int(shots * ((n_out + 7) // 8)),
                            "api": "B200ProgramSampler.sample_packed (ksim_program_sample_packed)"},
-            "roofline": {"bound": "alu", "achieved": achieved / 1e9, "peak": peak.value / 1e9,
-                         "unit": "Gop/s (int32)", "frac": achieved / peak.value,
-                         "traffic": (NCU_DRAM_BYTES_PER_SHOT[w.name] * shots
-                                     if w.name in NCU_DRAM_BYTES_PER_SHOT else None),
-                         "traffic_unit": "bytes per launch",
-                         "algorithmic_bytes": hbm_bytes,
-                         "ops_per_shot": work["ops"], "hbm_gbs": hbm_bytes / mean_s / 1e9,
-                         "peak_source": "ksim_measure_int_peak on this GPU (burst)"},
+            "roofline": roofline,
+            "parity": parity,
             "cpu_baseline": cpu,
+            "cpu_baseline_numpy": cpu_numpy,
+            "legs": legs,
             "batched": batched,
             "served": served,
-            "clocks": clk.summary(),
+            "clocks": clocks,
             "gpu_launches": args.steps * len(prog.components),
             "step_ms": step_ms,
         }

@@ -289,9 +289,11 @@ typedef struct ksim_batch_job {
 } ksim_batch_job;
 
 /* Launch shape of a batch (zero / negative fields take the defaults:
- * 128 threads, 16 KiB slots, CTAs per SM from occupancy, graph on). */
+ * 256 threads, 16 KiB slots, CTAs per SM from occupancy, graph on).  A work
+ * item is 2 x `threads` shots of a W <= 4 job (two shots per thread) and
+ * `threads` shots of a wider one. */
 typedef struct ksim_batch_tuning {
-    int32_t threads;      /* shots per work item (one per thread), multiple of 32, <= 256 */
+    int32_t threads;      /* threads per CTA (a multiple of 32, <= 256); see the item size above */
     int32_t slot_bytes;   /* staging slot, multiple of 16, >= every job's largest term */
     int32_t ctas_per_sm;  /* persistent CTAs per SM (<= occupancy limit) */
     int32_t use_graph;    /* 1: capture counter reset + kernels in a CUDA graph */
@@ -399,6 +401,11 @@ ksim_status ksim_work_model(const ksim_graph_desc *graphs, int32_t n_graphs, int
  * (32-bit add / shift / logic), in int32 lane-operations per second: the
  * roofline denominator of the sampling kernels.  No reference counterpart. */
 ksim_status ksim_measure_int_peak(int32_t device, double *ops_per_s, double *ms);
+/* Integer ALU throughput alone (three-input add and three-input logic
+ * chains, no shifts, multiplies or popcounts), in int32 lane-operations per
+ * second: the ceiling of the pure add / logic part of the sampler's work.
+ * No reference counterpart. */
+ksim_status ksim_measure_alu_peak(int32_t device, double *ops_per_s, double *ms);
 
 #ifdef __cplusplus
 }

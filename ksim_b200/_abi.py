@@ -218,6 +218,7 @@ def _declare(L: ctypes.CDLL) -> None:
         "ksim_program_sample_device": (i32, [vp, vp, i64, i64, i64, u64, i32, vp, vp]),
         "ksim_program_sample_packed": (i32, [vp, _u8p, i64, i64, u64, i32, _u8p]),
         "ksim_measure_int_peak": (i32, [i32, dp, dp]),
+        "ksim_measure_alu_peak": (i32, [i32, dp, dp]),
         "ksim_work_model": (i32, [ctypes.POINTER(GraphDesc), i32, i32, dp, i64p]),
         "ksim_batch_create": (i32, [ctypes.POINTER(BatchJob), i32, ctypes.POINTER(BatchTuning),
                                     ctypes.POINTER(vp)]),

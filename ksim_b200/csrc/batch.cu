@@ -40,15 +40,49 @@ struct BatchItem {
 
 namespace {
 
-// Class 0 runs W <= 4, class 1 the wider vectors (scratch sized for W = 16).
-size_t batch_smem_bytes(int slot_bytes, int cls, int threads)
+// Class 0 runs W <= 4, class 1 the wider vectors; the parity scratch is
+// sized for the largest W among a launch's jobs (smaller scratch leaves more
+// of the SM's shared storage to L1).
+size_t batch_smem_bytes(int slot_bytes, int max_w, int threads)
 {
-    return sample_smem_bytes(slot_bytes, true, cls == 0 ? 4 : 16, threads);
+    return sample_smem_bytes(slot_bytes, true, max_w, threads);
 }
 
+// One item's body per (W, term paths), each out of line: register-allocated
+// on its own, so the 32-bit and hybrid bodies keep the allocation of the
+// plain kernels compiled for those paths, and the general body (64-bit words,
+// exact path; rare) cannot raise it.  An item is a whole tile of shots, so
+// the call costs nothing measurable.
+// Shots per thread of an item: two for W <= 4 (one for the hybrid and
+// general bodies when KSIM_BATCH_WIDE_S is 1, for a smaller register budget),
+// one for wider vectors.
+#ifndef KSIM_BATCH_WIDE_S
+#define KSIM_BATCH_WIDE_S 2
+#endif
+__host__ __device__ constexpr int batch_spt(int W, int paths)
+{
+    return paths == PATHS_NARROW ? shots_per_thread(W) : (W <= 4 ? KSIM_BATCH_WIDE_S : 1);
+}
+
+template <int W, int PATHS>
+__device__ __noinline__ bool batch_tile(const SampleJob &j, int64_t s0, uint64_t *bar, uint8_t *slots, uint32_t &g,
+                                        uint8_t *scratch)
+{
+    return sample_tile<W, true, false, batch_spt(W, PATHS), PATHS>(j, s0, bar, slots, g, scratch);
+}
+
+// Class 0 (W <= 4): 128 registers, two CTAs of 256 threads per SM: on the
+// mixed benchmark batch (32-bit, hybrid and general bodies in one launch) the
+// fastest of the measured shapes (96 registers with five CTAs of 128, or with
+// one shot per thread for the hybrid bodies, ran 10-20 % slower); class 1
+// (W 5..16): the general body at up to 255.
+#ifndef KSIM_BATCH_MAXNREG
+#define KSIM_BATCH_MAXNREG 128
+#endif
+#define KSIM_BATCH_BOUNDS(C) __maxnreg__((C) == 0 ? KSIM_BATCH_MAXNREG : 255)
 template <int CLASS>
-__global__ void __launch_bounds__(256, CLASS == 0 ? KSIM_SAMPLE_MIN_CTAS : 1) k_batch(const BatchJobDev *__restrict__ jobs,
-                                               const BatchItem *__restrict__ items, int n_items, int *counter)
+__global__ void KSIM_BATCH_BOUNDS(CLASS) k_batch(const BatchJobDev *__restrict__ jobs,
+                                                 const BatchItem *__restrict__ items, int n_items, int *counter)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ int s_item;
@@ -67,14 +101,13 @@ __global__ void __launch_bounds__(256, CLASS == 0 ? KSIM_SAMPLE_MIN_CTAS : 1) k_
         const BatchJobDev &J = jobs[w.job];
         bool ok = true;
         if (CLASS == 0) {
-            // programs whose terms all run on 32-bit words take the kernel
-            // body compiled without the other paths
-#define KSIM_BATCH_W(WW)                                                                                  \
-    case WW:                                                                                              \
-        ok = J.paths == PATHS_NARROW                                                                      \
-                 ? sample_tile<WW, true, false, shots_per_thread(WW), PATHS_NARROW>(J.j, w.s0, bar, slots, g, \
-                                                                                   scratch)               \
-                 : sample_tile<WW, true, false, shots_per_thread(WW)>(J.j, w.s0, bar, slots, g, scratch); \
+            // each job takes the body compiled for the term paths it uses
+#define KSIM_BATCH_W(WW)                                                                              \
+    case WW:                                                                                          \
+        ok = J.paths == PATHS_NARROW ? batch_tile<WW, PATHS_NARROW>(J.j, w.s0, bar, slots, g, scratch) \
+             : J.paths == PATHS_NARROW_HYBRID                                                         \
+                 ? batch_tile<WW, PATHS_NARROW_HYBRID>(J.j, w.s0, bar, slots, g, scratch)            \
+                 : batch_tile<WW, PATHS_ALL>(J.j, w.s0, bar, slots, g, scratch);                     \
         break;
             switch (J.W) {
             KSIM_BATCH_W(1) KSIM_BATCH_W(2) KSIM_BATCH_W(3)
@@ -103,7 +136,8 @@ using namespace ksim;
 
 struct ksim_batch {
     int device = 0;
-    int threads = 128, slot_bytes = 16384, ctas_per_sm = 0, use_graph = 1;
+    int threads = 256, slot_bytes = 16384, ctas_per_sm = 0, use_graph = 1;
+    int max_w[2] = {1, 5};  // largest W among each class's jobs (parity scratch size)
     std::vector<ksim_component *> comps;
     std::vector<BatchJobDev> host_jobs;
     BatchJobDev *d_jobs = nullptr;
@@ -122,7 +156,7 @@ static ksim_status batch_enqueue(ksim_batch *b, cudaStream_t st)
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(work counter)");
     for (int cls = 0; cls < 2; ++cls) {
         if (!b->n_items[cls]) continue;
-        const size_t smem = batch_smem_bytes(b->slot_bytes, cls, b->threads);
+        const size_t smem = batch_smem_bytes(b->slot_bytes, b->max_w[cls], b->threads);
         if (cls == 0)
             k_batch<0><<<b->grid[0], b->threads, smem, st>>>(b->d_jobs, b->d_items[0], b->n_items[0], b->d_counter);
         else
@@ -151,7 +185,7 @@ ksim_status ksim_batch_create(const ksim_batch_job *jobs, int32_t n_jobs, const 
     }
     if (b->threads > 256 || (b->threads & 31))
         return fail(KSIM_ERR_INVALID_ARGUMENT, "threads must be a multiple of 32 in [32, 256]");
-    if ((b->slot_bytes & 15) || batch_smem_bytes(b->slot_bytes, 0, b->threads) > 227 * 1024)
+    if ((b->slot_bytes & 15) || batch_smem_bytes(b->slot_bytes, 4, b->threads) > 227 * 1024)
         return fail(KSIM_ERR_INVALID_ARGUMENT,
                     "slot_bytes must be a multiple of 16, and two slots with the parity scratch fit in 227 KiB");
     int device = -1;
@@ -209,7 +243,8 @@ ksim_status ksim_batch_create(const ksim_batch_job *jobs, int32_t n_jobs, const 
         double bytes = 0;
         for (const GraphDir &gd : c->img.gdir) bytes += (double)gd.stream_bytes + 64.0;
         const int cls = d.W <= 4 ? 0 : 1;
-        const int64_t tile = (int64_t)b->threads * shots_per_thread(d.W);
+        b->max_w[cls] = std::max(b->max_w[cls], d.W);
+        const int64_t tile = (int64_t)b->threads * batch_spt(d.W, d.paths);
         for (int64_t s0 = 0; s0 < jb.B; s0 += tile) {
             BatchItem it = {};
             it.job = i;
@@ -230,7 +265,7 @@ ksim_status ksim_batch_create(const ksim_batch_job *jobs, int32_t n_jobs, const 
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     for (int cls = 0; cls < 2; ++cls) {
-        const size_t smem = batch_smem_bytes(b->slot_bytes, cls, b->threads);
+        const size_t smem = batch_smem_bytes(b->slot_bytes, b->max_w[cls], b->threads);
         std::vector<int> order(items[cls].size());
         std::iota(order.begin(), order.end(), 0);
         std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[cls][x] > cost[cls][y]; });

@@ -136,7 +136,7 @@ double term_work(int W, uint32_t flags, const int n_cls[4], int n_hp, int n_pp, 
     double w = (double)sum_iter + 23.0 * nb;
     if (n_cls[1] | n_cls[3]) w += 16.0 * cn + 2.0;
     w += 4.0 * cn;
-    w += ((n_ph + 1) / 2) * (3.0 + 6.0 + 8.0 + 8.0 + 16.0 * c + 4.0 * c + 1.0);
+    w += ((n_ph + 1) / 2) * (3.0 + 5.0 + 8.0 + 8.0 + 16.0 * c + 4.0 * c + 1.0);
     w += 4.0 + (c == 1.0 ? 16.0 : 64.0) + 6.0 * c + 16.0;
     return w;
 }
@@ -468,14 +468,15 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 for (const auto &sv : ph_state) ref_max = std::max(ref_max, sv.second + std::log2(S) + 1e-12);
             // The fast path runs PhasePairs columns in pairs (zring.cuh): its
             // exact points are the unhalved pair products, then the end.  Pair tables: the 16
-            // products F F' and the factors' valuations, by folded signs.
+            // products F F' by folded signs, and the step table of the pair's
+            // halvings (see pair_step below).
             auto ph_factor = [&](size_t col, uint32_t k, int64_t f[4]) {
                 phase_pair((int)(ph_j[col].first | ((k & 1u) << 2)), (int)(ph_j[col].second | ((k >> 1) << 2)), f);
             };
             // (an odd last column pairs with the factor 1: valuation 0)
             const size_t n_pair = ((size_t)n_ph + 1) / 2;
             std::vector<uint8_t> pair_tab(64 * n_pair, 0);
-            std::vector<uint32_t> pair_nu(n_pair, 0);
+            std::vector<uint8_t> pair_step(256 * n_pair, 0);
             bool pair_ok = true;
             auto ph_factor2 = [&](size_t col, uint32_t k, int64_t f[4]) {
                 if (col < (size_t)n_ph) {
@@ -488,12 +489,34 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 std::map<uint32_t, double> fs;
                 fs[nu] = L_np;
                 for (size_t q = 0; q < n_pair; ++q) {
-                    for (uint32_t k = 0; k < 4; ++k) {
-                        int64_t f[4];
-                        ph_factor2(2 * q, k, f);
-                        pair_nu[q] |= std::min<uint32_t>(zw_valuation(f), 15u) << (4 * k);
-                        ph_factor2(2 * q + 1, k, f);
-                        pair_nu[q] |= std::min<uint32_t>(zw_valuation(f), 15u) << (16 + 4 * k);
+                    // step table: entry 16 c + nu (c = the pair's four sign
+                    // bits, nu = the valuation of z before the pair, 0..15)
+                    // holds the pair's halvings h1 + h2 (bits 0-1), nu after
+                    // it (bits 2-5) and whether z stays nonzero (bit 6): the
+                    // reference halves after a factor iff nu(z) >= 4, and a
+                    // zero factor stops the halvings from where it acts.  A
+                    // factor can have nu up to 6, so nu may grow; terms whose
+                    // reachable nu leaves 0..15 take the exact path.
+                    for (const auto &sv : fs)
+                        if (sv.first > 15) pair_ok = false;
+                    const uint32_t second = 2 * q + 1 < (size_t)n_ph ? 1u : 0u;
+                    for (uint32_t c = 0; c < 16; ++c) {
+                        int64_t f1[4], f2[4];
+                        ph_factor2(2 * q, c & 3u, f1);
+                        ph_factor2(2 * q + 1, c >> 2, f2);
+                        const uint32_t v1 = std::min<uint32_t>(zw_valuation(f1), 15u);
+                        const uint32_t v2 = std::min<uint32_t>(zw_valuation(f2), 15u);
+                        for (uint32_t nu0 = 0; nu0 < 16; ++nu0) {
+                            uint32_t alive = v1 != 15 ? 1u : 0u;
+                            uint32_t tt = nu0 + v1;
+                            const uint32_t h1 = (tt >= 4 ? 1u : 0u) & alive;
+                            alive &= v2 != 15 ? 1u : 0u;
+                            tt = tt - 4 * h1 + v2;
+                            const uint32_t h2 = (tt >= 4 ? 1u : 0u) & alive & second;
+                            const uint32_t nu1 = alive ? tt - 4 * h2 : 0u;
+                            if (nu1 > 15) continue;  // unreachable unless a state above is (then unsafe)
+                            pair_step[256 * q + 16 * c + nu0] = (uint8_t)((h1 + h2) | (nu1 << 2) | (alive << 6));
+                        }
                     }
                     std::map<uint32_t, double> next;
                     for (uint32_t c = 0; c < 16; ++c) {
@@ -524,6 +547,8 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                     }
                     fs.swap(next);
                 }
+                for (const auto &sv : fs)
+                    if (sv.first > 15) pair_ok = false;
                 if (S > 0)
                     for (const auto &sv : fs) fast_max = std::max(fast_max, sv.second + std::log2(S) + 1e-12);
             }
@@ -615,7 +640,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                     }
                 while (body.size() & 15u) body.push_back(0);
                 body.insert(body.end(), pair_tab.begin(), pair_tab.end());
-                for (uint32_t v : pair_nu) put32(body, v);
+                body.insert(body.end(), pair_step.begin(), pair_step.end());
                 while (body.size() & 15u) body.push_back(0);
                 nb = (uint32_t)((rows.size() + 31) / 32);
                 const uint16_t zero_off = (uint16_t)(8 * 64 * W);

@@ -59,7 +59,7 @@ struct ServeJob {
     int32_t W, n_tiles;
     int32_t next_tile;  // tiles handed out (atomic)
     int32_t remaining;  // tiles not finished (atomic)
-    int32_t req_slot, pad0;
+    int32_t req_slot, paths;  // paths: the component's term paths (LaunchCfg::paths)
     int64_t pad1;
 };
 static_assert(sizeof(SampleJob) % 16 == 0, "SampleJob is copied in 16-byte words");
@@ -97,12 +97,24 @@ __device__ __forceinline__ T vload(const T *p)
     return *(const volatile T *)p;
 }
 
+// One tile of a job with the body compiled for the job's term paths, out of
+// line so each body keeps its own register allocation (the 32-bit and
+// hybrid bodies carry almost all work; the general one is rare).  Job data
+// comes through L2-only loads (CG): buffers are reused across requests
+// within one kernel lifetime.
+template <int W, int PATHS>
+__device__ __noinline__ bool serve_tile(const SampleJob &j, int64_t s0, uint64_t *bar, uint8_t *slots, uint32_t &g,
+                                        uint8_t *scratch)
+{
+    return sample_tile<W, true, true, shots_per_thread(W), PATHS>(j, s0, bar, slots, g, scratch);
+}
+
 __global__ void __launch_bounds__(256, KSIM_SAMPLE_MIN_CTAS) k_serve(ServeJob *jobs, ServeReqDev *reqs, const unsigned long long *ring,
                                                int ring_cap, ServeCtl *ctl, uint32_t *done_flags, long long idle_ns)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ __align__(16) SampleJob s_job;
-    __shared__ int s_slot, s_tile, s_W;
+    __shared__ int s_slot, s_tile, s_W, s_paths;
     uint64_t *bar = (uint64_t *)smem;
     uint8_t *slots = smem + BAR_BYTES;
     ring_init(bar);
@@ -129,6 +141,7 @@ __global__ void __launch_bounds__(256, KSIM_SAMPLE_MIN_CTAS) k_serve(ServeJob *j
                 backoff = 64;
                 *(volatile long long *)&ctl->last_claim_ns = global_ns();
                 s_W = vload(&jobs[slot].W);
+                s_paths = vload(&jobs[slot].paths);
             } else {
                 const long long now = global_ns();
                 const long long last = vload(&ctl->last_claim_ns);
@@ -158,12 +171,19 @@ __global__ void __launch_bounds__(256, KSIM_SAMPLE_MIN_CTAS) k_serve(ServeJob *j
             const int64_t s0 = (int64_t)s_tile * blockDim.x * S;
             uint8_t *scratch = slots + (size_t)NSLOT * s_job.slot_bytes;
             bool ok;
+            const int paths = s_paths;
+#define KSIM_SERVE_W(WW)                                                                                \
+    case WW:                                                                                            \
+        ok = paths == PATHS_NARROW ? serve_tile<WW, PATHS_NARROW>(s_job, s0, bar, slots, g, scratch)    \
+             : paths == PATHS_NARROW_HYBRID                                                             \
+                 ? serve_tile<WW, PATHS_NARROW_HYBRID>(s_job, s0, bar, slots, g, scratch)              \
+                 : serve_tile<WW, PATHS_ALL>(s_job, s0, bar, slots, g, scratch);                       \
+        break;
             switch (s_W) {
-            case 1: ok = sample_tile<1, true, true, S>(s_job, s0, bar, slots, g, scratch); break;
-            case 2: ok = sample_tile<2, true, true, S>(s_job, s0, bar, slots, g, scratch); break;
-            case 3: ok = sample_tile<3, true, true, S>(s_job, s0, bar, slots, g, scratch); break;
-            default: ok = sample_tile<4, true, true, S>(s_job, s0, bar, slots, g, scratch); break;
+            KSIM_SERVE_W(1) KSIM_SERVE_W(2) KSIM_SERVE_W(3)
+            default: KSIM_SERVE_W(4)
             }
+#undef KSIM_SERVE_W
             __threadfence();  // this thread's outputs before the counters below
             __syncthreads();
             if (threadIdx.x == 0) {
@@ -356,6 +376,7 @@ ksim_status admit(ksim_server *s, ServeRequest *r)
         J.j.seed = r->seed + 0x9E37ull * (uint64_t)k;
         J.j.status = &s->d_reqs[r->slot].flags;
         J.W = c->img.W;
+        J.paths = c->cfg.paths;
         J.n_tiles = (int32_t)tiles;
         J.next_tile = 0;
         J.remaining = (int32_t)tiles;

@@ -427,20 +427,19 @@ KS_HD int term_meta_off(const TermHdr &h) { return TERM_HDR_BYTES + ((h.flags & 
 constexpr int TERM_FFK_BYTES = 128;
 // PhasePairs columns 2p and 2p + 1 run as one pair (an odd last column
 // pairs with the factor 1, its sign bits being rows past the end, which are
-// zero): a table of the 16 products (4 x i8 each, combo = pa | pb << 1 |
-// pa' << 2 | pb' << 3) and a word of the two factors' (1 - w)-adic
-// valuations per sign pair (nibble k = factor 1 for pa | pb << 1 = k,
-// nibble 4 + k = factor 2; 15 = the factor is 0).
+// zero): a table of the 16 products (4 x i8 each, combo c = pa | pb << 1 |
+// pa' << 2 | pb' << 3), then per pair a 256-byte step table: entry 16 c + nu,
+// for the valuation nu (0..15; a factor can have nu up to 6, so nu can grow,
+// and the packer sends terms that can leave that range to the exact path) of
+// z before the pair, holds the pair's halvings (bits 0-1), the valuation
+// after it (bits 2-5) and whether z stays nonzero (bit 6).
 KS_HD uint32_t term_ph_pairs(const TermHdr &h) { return (h.n_ph + 1) >> 1; }
 KS_HD int term_pair_tab_off(const TermHdr &h)
 {
     return term_meta_off(h) + TERM_FFK_BYTES + ((2 * (int)h.n_cls[0] + 15) & ~15);
 }
-KS_HD int term_pair_nu_off(const TermHdr &h) { return term_pair_tab_off(h) + 64 * (int)term_ph_pairs(h); }
-KS_HD int term_blocks_off(const TermHdr &h)
-{
-    return term_pair_nu_off(h) + ((4 * (int)term_ph_pairs(h) + 15) & ~15);
-}
+KS_HD int term_pair_step_off(const TermHdr &h) { return term_pair_tab_off(h) + 64 * (int)term_ph_pairs(h); }
+KS_HD int term_blocks_off(const TermHdr &h) { return term_pair_step_off(h) + 256 * (int)term_ph_pairs(h); }
 KS_HD void load_i32x4(const uint8_t *p, int32_t (&r)[4])
 {
 #if defined(__CUDA_ARCH__)
@@ -609,39 +608,33 @@ KS_HD const uint8_t *eval_term_rows(const uint8_t *p, const TermHdr &h, const Ro
     const int ph0 = term_ph_row0(h);
     // PhasePairs in pairs: the valuation of z (known per shot: the
     // NodePhases result has nu = (2 n2 + n1 + n3) mod 4, and each factor's nu
-    // is tabulated) decides the reference's two halvings, so one product
-    // with the tabulated F F' and one shift replace two factors and two
-    // evenness tests.  A zero factor leaves z = 0 and no halving after it.
+    // is fixed by its signs) decides the reference's two halvings, so one
+    // product with the tabulated F F' and one shift replace two factors and
+    // two evenness tests; the pair's step table gives the halvings, the next
+    // nu and whether a zero factor ended the halvings, from (signs, nu).
     {
         const uint32_t n_pair = term_ph_pairs(h);
         const uint8_t *ptab = p + term_pair_tab_off(h);
-        const uint32_t *pnu = (const uint32_t *)(p + term_pair_nu_off(h));
+        const uint8_t *pstep = p + term_pair_step_off(h);
         uint32_t nu[S];
 #pragma unroll
         for (int s = 0; s < S; ++s) nu[s] = (2u * h.n_cls[1] + h.n_cls[2] + h.n_cls[3]) & 3u;
         for (uint32_t q = 0; q < n_pair; ++q) {
-            const uint32_t nuw = pnu[q];
             const int pos = ph0 + 4 * (int)q;
-            const uint32_t second = 2 * q + 1 < h.n_ph ? 1u : 0u;  // the factor 1 takes no step
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 const uint32_t c = (bits[s].word(pos >> 5) >> (pos & 31)) & 15u;
-                const uint32_t v1 = (nuw >> (4u * (c & 3u))) & 15u, v2 = (nuw >> (16u + 4u * (c >> 2))) & 15u;
-                // a zero factor stops the halvings from where it acts: the
-                // first factor's halving still happens if only the second is 0
-                alive[s] &= v1 != 15u ? 1u : 0u;
-                uint32_t t = nu[s] + v1;
-                const uint32_t h1 = (t >= 4u ? 1u : 0u) & alive[s];
-                alive[s] &= v2 != 15u ? 1u : 0u;
-                t = t - 4u * h1 + v2;
-                const uint32_t h2 = (t >= 4u ? 1u : 0u) & alive[s] & second;
-                nu[s] = t - 4u * h2;
+                const uint32_t e = pstep[256 * q + 16 * c + nu[s]];
+                // a term already zero (class-0 kill, earlier zero factor) takes no halving
+                const uint32_t hh = e & 3u & (0u - alive[s]);
+                alive[s] &= e >> 6;
+                nu[s] = (e >> 2) & 15u;
                 const uint32_t fw = *(const uint32_t *)(ptab + 64 * q + 4 * c);  // 4 x i8
                 const Zr<T> F = {(T)(int64_t)((int32_t)(fw << 24) >> 24), (T)(int64_t)((int32_t)(fw << 16) >> 24),
                                  (T)(int64_t)((int32_t)(fw << 8) >> 24), (T)(int64_t)((int32_t)fw >> 24)};
                 z[s] = zmul(z[s], F);
-                shr_all(z[s], h1 + h2);
-                pw[s] += (int32_t)(h1 + h2);
+                shr_all(z[s], hh);
+                pw[s] += (int32_t)hh;
             }
         }
     }

@@ -35,6 +35,35 @@ def component_work(comp) -> dict:
             "exact_terms": paths[2], "hybrid_terms": paths[3]}
 
 
+def reference_op_model(prog) -> float:
+    """int32 operations per shot of the reference's own algorithm
+    (zx_eval.hpp:75-181 run once per graph, kokkos_sim.cpp:214-230): per
+    term g of graph k, cnt_np[g] + cnt_ph[g] + 3 Z[w] products (NodePhases and
+    PhasePairs columns, HalfPi, prefactor phase, floatfactor) at 84 int32 ops
+    each (16 int64 multiplies at 3, 12 int64 adds at 2, the reduce at 12), and
+    (Tnp + Thp + 2 Tpp + 2 Tph) * ceil(P_k / 64) 64-bit parity words at 5 ops
+    each (AND, POPC and accumulate on 64-bit words).  It describes the
+    reference's step-by-step work, not the reformulated work the kernels run
+    (``component_work``), which is several times smaller."""
+    total = 0.0
+    for comp in prog.components:
+        for g in comp.graphs:
+            G = int(g.pf_phase_idx.shape[0])
+            if G == 0:
+                continue
+            Tnp = int(g.np_phases.shape[1]) if g.np_phases.ndim > 1 else 0
+            Thp = int(g.hp_coeffs.shape[1]) if g.hp_coeffs.ndim > 1 else 0
+            Tpp = int(g.pp_psi_c.shape[1]) if g.pp_psi_c.ndim > 1 else 0
+            Tph = int(g.ph_alpha.shape[1]) if g.ph_alpha.ndim > 1 else 0
+            P = int(g.np_params.shape[2]) if g.np_params.ndim > 2 else 0
+            words = max(1, -(-P // 64))
+            zmul = float(np.sum(np.asarray(g.np_counts, np.int64)) +
+                         np.sum(np.asarray(g.ph_counts, np.int64)) + 3 * G)
+            parw = float(G * (Tnp + Thp + 2 * Tpp + 2 * Tph) * words)
+            total += 84.0 * zmul + 5.0 * parw
+    return total
+
+
 def program_work(prog) -> dict:
     """Per-shot totals over all components and graphs of a FlatProgram."""
     tot = {"terms": 0, "ops": 0.0, "graphs": 0, "in_bytes": 0, "out_bytes": 0,
