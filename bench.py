@@ -71,6 +71,9 @@ NCU_DRAM_BYTES_PER_SHOT = {"cfg2-medium-40q-t12": 66.2 + 40.0}
 # launch); the issue roofline of the bench line is this times shots/s over
 # the SMs' issue ceiling.  Source: profiles/k_sample_cfg2_current.md.
 NCU_THREAD_INST_PER_SHOT = {}
+# Gate locations of the workloads' circuits (qubits x depth): one
+# single-qubit Pauli channel each in the noisy end-to-end leg.
+NOISE_LOCATIONS = {"cfg2-medium-40q-t12": 40 * 200, "cfg4-large-rank-85q-t20": 85 * 600}
 
 
 def parse():
@@ -690,7 +693,10 @@ def main():
     # (one channel per gate location), then sampled: only outputs cross PCIe
     from ksim_b200 import synth
     from ksim_b200.noise import DeviceChannelSampler
-    nprobs, nT = synth.noise_model(np.random.default_rng(w.seed + 7), n_f, 200)
+    # (the medium circuit: 40 qubits x depth 200 = 8,000 single-qubit Pauli
+    # locations, X/Y/Z each p = 1e-3)
+    n_loc = NOISE_LOCATIONS.get(w.name, 200)
+    nprobs, nT = synth.noise_model(np.random.default_rng(w.seed + 7), n_f, n_loc)
     noise = DeviceChannelSampler(nprobs, nT, seed=w.seed, device=local)
     for i in range(max(1, args.warmup)):
         sampler.sample_noisy(noise, shots, 3000 + i, rng_mode=args.rng, out=out_pin)
@@ -779,7 +785,8 @@ def main():
             "e2e_noisy": {"value": e2n_value, "unit": "shots/s", "h2d_bytes_per_step": 0,
                           "d2h_bytes_per_step": int(shots * n_out),
                           "api": "B200ProgramSampler.sample_noisy (ksim_program_sample_noisy): "
-                                 "f drawn on the device from 200 Pauli channels"},
+                                 f"f drawn on the device from {n_loc} Pauli channels "
+                                 f"({noise.num_channels} after merging)"},
             "e2e_packed": {"value": e2p_value, "unit": "shots/s",
                            "h2d_bytes_per_step": int(fp_pin.nbytes),
                            "d2h_bytes_per_step": int(shots * ((n_out + 7) // 8)),

@@ -243,19 +243,24 @@ ksim_status ksim_program_sample_device(ksim_program *p, const uint8_t *d_f_param
  * (src/python/ksim/compile/channels.py:531-576).  Channel i has n_bits[i]
  * error bits and 2^n_bits[i] outcome probabilities, concatenated in `probs`
  * (outcome index bit b = error bit b, channels.py:12-24); error_transform is
- * (num_f, num_e) uint8 row-major, num_e = sum of n_bits.  The draw
- * (ChannelSampler.sample, channels.py:624-658) runs one thread per shot over
- * all channels with counter-based Philox4x32-10 draws keyed by (seed, shot):
- * channel c fires iff u32(shot, c) < floor(p_fire 2^32), the outcome is the
- * first whose conditional-CDF threshold exceeds a second draw, and its f
- * pattern is XORed in. */
+ * (num_f, num_e) uint8 row-major, num_e = sum of n_bits.  At creation,
+ * channels that never fire are dropped and channels over identical
+ * error-bit patterns are merged by XOR convolution (channels.py:398-429); the
+ * rest are ordered by firing probability into runs of equal p, each with
+ * integer skip thresholds floor((1 - p)^k 2^32).  The draw
+ * (ChannelSampler.sample, channels.py:624-658) runs one thread per shot with
+ * one counter-based Philox4x32-10 stream keyed by (seed, shot): within a run
+ * the next firing channel is j + 1 + #{k : u < T_k} for a fresh draw u, the
+ * outcome is the first whose conditional-CDF threshold exceeds the next draw,
+ * and its f pattern is XORed in; the work per shot follows the channels that
+ * fire. */
 typedef struct ksim_noise ksim_noise;
 ksim_status ksim_noise_create(const double *probs, const int32_t *n_bits, int32_t n_channels,
                               const uint8_t *error_transform, int32_t num_f, int32_t num_e,
                               int32_t device, ksim_noise **out);
 void ksim_noise_destroy(ksim_noise *n);
 int32_t ksim_noise_num_f(const ksim_noise *n);
-int32_t ksim_noise_num_channels(const ksim_noise *n);   /* channels that can fire */
+int32_t ksim_noise_num_channels(const ksim_noise *n);   /* channels that can fire, after merging */
 /* f rows (B x num_f bytes, f_stride apart) for shots shot_offset.. on the device. */
 ksim_status ksim_noise_sample_device(ksim_noise *n, int64_t B, int64_t shot_offset, uint64_t seed,
                                      uint8_t *d_f, int64_t f_stride, void *stream);

@@ -4,14 +4,18 @@
 arguments of the reference's ``ChannelSampler``
 (``src/python/ksim/compile/channels.py:531-576``) and its ``sample(n)``
 returns the same kind of (n, num_f) uint8 matrix
-(``channels.py:624-658``), drawn by ``ksim_noise_*`` kernels.  The draw is
-counter-based (Philox4x32-10 keyed by (seed, shot)): channel c fires in shot
-s iff a 32-bit draw is below floor(p_fire * 2^32), a second draw picks the
-outcome from the conditional CDF, and the outcome's f pattern is XORed in.
-Per channel the probabilities equal the reference's to within 2^-32, and
-channels are independent as in the reference, so the distribution of f is
-the reference's; the streams differ (the reference uses numpy's PCG64 with
-geometric skips).
+(``channels.py:624-658``), drawn by ``ksim_noise_*`` kernels.  At creation
+channels over identical error-bit patterns are merged by XOR convolution
+(the reference's ``merge_identical_channels``, ``channels.py:398-429``) and
+channels of equal firing probability form runs.  The draw is counter-based
+(one Philox4x32-10 stream per shot keyed by (seed, shot)): within a run the
+next firing channel is found by a geometric skip (one draw, integer
+thresholds floor((1 - p)^k 2^32)), a second draw picks the outcome from the
+conditional CDF, and the outcome's f pattern is XORed in, so the work per
+shot follows the channels that fire.  Per channel the probabilities equal the
+reference's to within 2^-32 per threshold, and channels are independent as
+in the reference, so the distribution of f is the reference's; the streams
+differ (the reference uses numpy's PCG64 with geometric skips along shots).
 
 ``B200ProgramSampler.sample_noisy`` draws f on the device and samples from it
 in one pipelined call: only the outputs cross PCIe.
@@ -104,7 +108,7 @@ class DeviceChannelSampler:
 
     @property
     def num_channels(self) -> int:
-        """Channels that can fire."""
+        """Channels that can fire, after merging identical signatures."""
         return int(self._L.ksim_noise_num_channels(self._h))
 
     def sample(self, num_samples: int = 1) -> np.ndarray:

@@ -324,14 +324,19 @@ int oracle_max_threads(void)
 
 /* ---- noise draw ----------------------------------------------------------
  * CPU restatement of the device noise draw (ksim_b200/csrc/noise.cu), the
- * checker for it: per shot, channel c fires iff word c%4 of
- * Philox(seed, (shot lo, shot hi, c/4, 'NOIS')) < floor(p_fire 2^32); a firing
- * channel's outcome is the first o whose threshold floor(cdf_o 2^32) exceeds
- * word 0 of Philox(seed, (shot lo, shot hi, c, 'OUTK')); its f pattern (XOR
- * of the error_transform columns of the outcome's error bits) is XORed in.
- * The model follows ChannelSampler._precompute_sparse (compile/channels.py:
- * 579-622): p_fire = 1 - probs[0], channels with p_fire <= 1e-15 never fire,
- * conditional CDF cumsum(probs[1:] / p_fire) normalised by its last entry. */
+ * checker for it.  The model follows ChannelSampler (compile/channels.py:
+ * 480-622): channels with p_fire = 1 - probs[0] <= 1e-15 never fire;
+ * channels over identical error-bit patterns (same bit count, same
+ * error_transform columns in order) are merged by XOR convolution, in order
+ * of first appearance; the conditional CDF is cumsum(probs[1:] / p_fire)
+ * normalised by its last entry.  The merged channels are ordered by p_fire
+ * (descending, ties in merged order) and cut into runs of equal p_fire, each
+ * with the table T_k = floor((1 - p)^k 2^32), k = 1.. (while > 0, at most the
+ * run's length).  Per shot, a stream of 32-bit draws (Philox4x32-10, key =
+ * seed, counter = (shot lo, shot hi, block, 'NOIS'), four words a block, in
+ * order) drives, per run, jumps from channel j to j + 1 + #{k : u < T_k};
+ * a channel jumped to fires with the first outcome o whose threshold
+ * floor(cdf_o 2^32) exceeds the next draw, and its f pattern is XORed in. */
 static uint32_t noise_threshold32(double u)
 {
     if (!(u > 0.0)) return 0u;
@@ -339,71 +344,167 @@ static uint32_t noise_threshold32(double u)
     return t >= 4294967295.0 ? 4294967295u : (uint32_t)t;
 }
 
+typedef struct {
+    int k;
+    double *p;       /* 2^k outcome probabilities */
+    uint64_t *bits;  /* k patterns of nw words */
+} nz_chan;
+
+typedef struct {
+    double p;
+    int idx;
+} nz_key;
+
+static int nz_cmp(const void *a, const void *b)
+{
+    const nz_key *x = (const nz_key *)a, *y = (const nz_key *)b;
+    if (x->p != y->p) return x->p > y->p ? -1 : 1;
+    return x->idx < y->idx ? -1 : x->idx > y->idx ? 1 : 0;
+}
+
+typedef struct {
+    uint64_t shot, seed;
+    uint32_t blk, pos, buf[4];
+} nz_stream;
+
+static uint32_t nz_next(nz_stream *st)
+{
+    if (st->pos == 4) {
+        uint32_t ctr[4] = {(uint32_t)st->shot, (uint32_t)(st->shot >> 32), st->blk++, 0x4E4F4953u};
+        uint32_t key[2] = {(uint32_t)st->seed, (uint32_t)(st->seed >> 32)};
+        oracle_philox4x32_10(ctr, key, st->buf);
+        st->pos = 0;
+    }
+    return st->buf[st->pos++];
+}
+
 int oracle_noise_sample(const double *probs, const int32_t *n_bits, int n_channels, const uint8_t *transform,
                         int num_f, int num_e, int64_t B, int64_t shot_offset, uint64_t seed, uint8_t *out)
 {
-    const uint32_t TAG_FIRE = 0x4E4F4953u, TAG_OUTCOME = 0x4F55544Bu;
-    uint32_t *thr = (uint32_t *)calloc((size_t)(n_channels > 0 ? n_channels : 1), sizeof(uint32_t));
-    int64_t *poff = (int64_t *)calloc((size_t)(n_channels > 0 ? n_channels : 1), sizeof(int64_t));
-    int *eoff = (int *)calloc((size_t)(n_channels > 0 ? n_channels : 1), sizeof(int));
-    int *fires = (int *)calloc((size_t)(n_channels > 0 ? n_channels : 1), sizeof(int));
-    uint32_t **cdf = (uint32_t **)calloc((size_t)(n_channels > 0 ? n_channels : 1), sizeof(uint32_t *));
-    if (!thr || !poff || !eoff || !fires || !cdf) return 1;
+    const int nw = num_f > 0 ? (num_f + 63) / 64 : 1;
+    uint64_t *col = (uint64_t *)calloc((size_t)(num_e > 0 ? num_e : 1) * nw, sizeof(uint64_t));
+    nz_chan *m = (nz_chan *)calloc((size_t)(n_channels > 0 ? n_channels : 1), sizeof(nz_chan));
+    if (!col || !m) return 1;
+    for (int fi = 0; fi < num_f; ++fi)
+        for (int e = 0; e < num_e; ++e)
+            if (transform[(size_t)fi * num_e + e]) col[(size_t)e * nw + fi / 64] |= 1ull << (fi % 64);
+    /* drop never-firing channels, merge identical signatures */
+    int n_m = 0;
     int64_t po = 0;
     int eo = 0;
     for (int i = 0; i < n_channels; ++i) {
-        const int64_t n = (int64_t)1 << n_bits[i];
+        const int k = n_bits[i];
+        const int64_t n = (int64_t)1 << k;
         const double *pr = probs + po;
-        poff[i] = po;
-        eoff[i] = eo;
+        const int e0 = eo;
         po += n;
-        eo += n_bits[i];
-        const double p_fire = 1.0 - pr[0];
-        if (!(p_fire > 1e-15) || n <= 1) continue;
-        fires[i] = 1;
-        thr[i] = noise_threshold32(p_fire);
-        cdf[i] = (uint32_t *)calloc((size_t)n, sizeof(uint32_t));
-        double *cum = (double *)calloc((size_t)n, sizeof(double));
-        double run = 0;
-        for (int64_t o = 1; o < n; ++o) {
-            run += (pr[o] > 0.0 ? pr[o] : 0.0) / p_fire;
-            cum[o - 1] = run;
+        eo += k;
+        if (!(1.0 - pr[0] > 1e-15) || n <= 1) continue;
+        int hit = -1;
+        for (int j = 0; j < n_m && hit < 0; ++j) {
+            if (m[j].k != k) continue;
+            int same = 1;
+            for (int b = 0; b < k && same; ++b)
+                for (int w = 0; w < nw; ++w)
+                    if (m[j].bits[(size_t)b * nw + w] != col[(size_t)(e0 + b) * nw + w]) { same = 0; break; }
+            if (same) hit = j;
         }
-        for (int64_t o = 0; o + 1 < n - 1; ++o) cdf[i][o] = noise_threshold32(cum[o] / cum[n - 2]);
-        free(cum);
+        if (hit >= 0) {
+            double *cv = (double *)calloc((size_t)n, sizeof(double));
+            for (int64_t a = 0; a < n; ++a)
+                for (int64_t b = 0; b < n; ++b) cv[a ^ b] += m[hit].p[a] * pr[b];
+            free(m[hit].p);
+            m[hit].p = cv;
+        } else {
+            m[n_m].k = k;
+            m[n_m].p = (double *)malloc(sizeof(double) * (size_t)n);
+            memcpy(m[n_m].p, pr, sizeof(double) * (size_t)n);
+            m[n_m].bits = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)(k > 0 ? k : 1) * nw);
+            memcpy(m[n_m].bits, col + (size_t)e0 * nw, sizeof(uint64_t) * (size_t)k * nw);
+            ++n_m;
+        }
     }
-    /* the device walks the firing channels only, numbered in order */
-    int *idx = (int *)calloc((size_t)(n_channels > 0 ? n_channels : 1), sizeof(int));
+    /* order by p_fire, runs, skip tables, CDF thresholds, outcome patterns */
+    nz_key *ord = (nz_key *)calloc((size_t)(n_m > 0 ? n_m : 1), sizeof(nz_key));
     int n_live = 0;
-    for (int i = 0; i < n_channels; ++i)
-        if (fires[i]) idx[n_live++] = i;
-    uint8_t *f = (uint8_t *)calloc((size_t)(num_f > 0 ? num_f : 1), 1);
+    for (int j = 0; j < n_m; ++j)
+        if (1.0 - m[j].p[0] > 1e-15) {
+            ord[n_live].p = 1.0 - m[j].p[0];
+            ord[n_live].idx = j;
+            ++n_live;
+        }
+    qsort(ord, (size_t)n_live, sizeof(nz_key), nz_cmp);
+    int *run_first = (int *)calloc((size_t)(n_live > 0 ? n_live : 1), sizeof(int));
+    int *run_n = (int *)calloc((size_t)(n_live > 0 ? n_live : 1), sizeof(int));
+    uint32_t **run_tab = (uint32_t **)calloc((size_t)(n_live > 0 ? n_live : 1), sizeof(uint32_t *));
+    int *run_len = (int *)calloc((size_t)(n_live > 0 ? n_live : 1), sizeof(int));
+    uint32_t **cdf = (uint32_t **)calloc((size_t)(n_live > 0 ? n_live : 1), sizeof(uint32_t *));
+    uint64_t **pat = (uint64_t **)calloc((size_t)(n_live > 0 ? n_live : 1), sizeof(uint64_t *));
+    int n_runs = 0;
+    for (int r0 = 0; r0 < n_live;) {
+        int r1 = r0;
+        while (r1 < n_live && ord[r1].p == ord[r0].p) ++r1;
+        run_first[n_runs] = r0;
+        run_n[n_runs] = r1 - r0;
+        run_tab[n_runs] = (uint32_t *)calloc((size_t)(r1 - r0), sizeof(uint32_t));
+        const double q = 1.0 - ord[r0].p;
+        double t = 1.0;
+        int len = 0;
+        for (int k = 1; k <= r1 - r0; ++k) {
+            t *= q;
+            const uint32_t thr = noise_threshold32(t);
+            if (thr == 0) break;
+            run_tab[n_runs][len++] = thr;
+        }
+        run_len[n_runs] = len;
+        for (int x = r0; x < r1; ++x) {
+            const nz_chan *c = &m[ord[x].idx];
+            const int64_t n = (int64_t)1 << c->k;
+            const double p_fire = ord[x].p;
+            double *cum = (double *)calloc((size_t)n, sizeof(double));
+            double run = 0;
+            for (int64_t o = 1; o < n; ++o) {
+                run += (c->p[o] > 0.0 ? c->p[o] : 0.0) / p_fire;
+                cum[o - 1] = run;
+            }
+            cdf[x] = (uint32_t *)calloc((size_t)n, sizeof(uint32_t));
+            for (int64_t o = 0; o + 1 < n - 1; ++o) cdf[x][o] = noise_threshold32(cum[o] / cum[n - 2]);
+            free(cum);
+            pat[x] = (uint64_t *)calloc((size_t)n * nw, sizeof(uint64_t));
+            for (int64_t o = 1; o < n; ++o)
+                for (int b = 0; b < c->k; ++b)
+                    if ((o >> b) & 1)
+                        for (int w = 0; w < nw; ++w) pat[x][(size_t)(o - 1) * nw + w] ^= c->bits[(size_t)b * nw + w];
+        }
+        ++n_runs;
+        r0 = r1;
+    }
+    uint64_t *acc = (uint64_t *)calloc((size_t)nw, sizeof(uint64_t));
     for (int64_t s = 0; s < B; ++s) {
-        const uint64_t shot = (uint64_t)(shot_offset + s);
-        memset(f, 0, (size_t)(num_f > 0 ? num_f : 1));
-        for (int c = 0; c < n_live; ++c) {
-            uint32_t ctr[4] = {(uint32_t)shot, (uint32_t)(shot >> 32), (uint32_t)(c / 4), TAG_FIRE};
-            uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
-            uint32_t x[4];
-            oracle_philox4x32_10(ctr, key, x);
-            const int ch = idx[c];
-            if (x[c % 4] >= thr[ch]) continue;
-            uint32_t ctr2[4] = {(uint32_t)shot, (uint32_t)(shot >> 32), (uint32_t)c, TAG_OUTCOME};
-            uint32_t y[4];
-            oracle_philox4x32_10(ctr2, key, y);
-            const int64_t n_out = ((int64_t)1 << n_bits[ch]) - 1;
-            int64_t o = 0;
-            while (o + 1 < n_out && y[0] >= cdf[ch][o]) ++o;
-            const int64_t outcome = o + 1; /* index into the channel's probs */
-            for (int b = 0; b < n_bits[ch]; ++b) {
-                if (!((outcome >> b) & 1)) continue;
-                const int e = eoff[ch] + b;
-                for (int fi = 0; fi < num_f; ++fi) f[fi] ^= transform[(size_t)fi * num_e + e];
+        nz_stream st = {(uint64_t)(shot_offset + s), seed, 0u, 4u, {0, 0, 0, 0}};
+        memset(acc, 0, sizeof(uint64_t) * (size_t)nw);
+        for (int r = 0; r < n_runs; ++r) {
+            int64_t j = -1;
+            for (;;) {
+                const uint32_t u = nz_next(&st);
+                int64_t kk = 0;
+                while (kk < run_len[r] && u < run_tab[r][kk]) ++kk; /* #{k : u < T_k}, T decreasing */
+                j += kk + 1;
+                if (j >= run_n[r]) break;
+                const int x = run_first[r] + (int)j;
+                const int64_t n_out = ((int64_t)1 << m[ord[x].idx].k) - 1;
+                const uint32_t v = nz_next(&st);
+                int64_t o = 0;
+                while (o + 1 < n_out && v >= cdf[x][o]) ++o;
+                for (int w = 0; w < nw; ++w) acc[w] ^= pat[x][(size_t)o * nw + w];
             }
         }
-        memcpy(out + s * num_f, f, (size_t)num_f);
+        for (int fi = 0; fi < num_f; ++fi) out[s * num_f + fi] = (uint8_t)((acc[fi / 64] >> (fi % 64)) & 1u);
     }
-    for (int i = 0; i < n_channels; ++i) free(cdf[i]);
-    free(cdf); free(thr); free(poff); free(eoff); free(fires); free(idx); free(f);
+    for (int x = 0; x < n_live; ++x) { free(cdf[x]); free(pat[x]); }
+    for (int r = 0; r < n_runs; ++r) free(run_tab[r]);
+    for (int j = 0; j < n_m; ++j) { free(m[j].p); free(m[j].bits); }
+    free(col); free(m); free(ord); free(run_first); free(run_n); free(run_tab); free(run_len);
+    free(cdf); free(pat); free(acc);
     return 0;
 }

@@ -74,3 +74,21 @@ def test_noise_edge_cases(cuda_device, oracle_port):
     s = B200ProgramSampler(prog, device=0)
     assert np.array_equal(s.sample_noisy(nof, 777, 5), s.sample(np.zeros((777, 0), np.uint8), 5))
     assert s.sample_noisy(nof, 0, 5).shape == (0, prog.num_outputs)
+
+
+def test_device_draw_long_runs_and_merges(cuda_device, oracle_port):
+    """A gate-level Pauli model of cfg2's size (8,000 locations, one long run
+    of equal firing probability), duplicated signatures that merge, channels
+    that always fire and a tiny-probability run: device rows equal the
+    oracle's, and the merged model has fewer channels."""
+    from ksim_b200.noise import DeviceChannelSampler
+    rng = np.random.default_rng(8000)
+    probs, T = synth.noise_model(rng, 64, 8000)
+    probs = list(probs) + [np.array([1 - 3e-3, 1e-3, 1e-3, 1e-3])] * 50 + [np.array([0.0, 1.0])] * 3 \
+        + [np.array([1 - 1e-9, 1e-9])] * 5
+    extra = [T[:, :2]] * 50 + [T[:, 2:3]] * 3 + [T[:, 3:4]] * 5
+    T = np.hstack([T] + extra)
+    ns = DeviceChannelSampler(probs, T, seed=99)
+    assert ns.num_channels < len(probs)
+    for B, off in ((3000, 0), (1000, 10**9)):
+        assert np.array_equal(ns.sample_at(B, off), oracle_port.noise_sample(probs, T, B, off, 99)), (B, off)

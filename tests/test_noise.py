@@ -82,3 +82,27 @@ def test_model_validation():
         _model_arrays([np.array([0.5, 0.3, 0.2])], np.zeros((2, 2), np.uint8))
     with pytest.raises(ValueError):
         _model_arrays([np.array([0.9, 0.1])], np.zeros((2, 3), np.uint8))
+
+
+def test_merged_channels_and_long_runs_hit_exact(oracle_port):
+    """Channels over identical error-bit patterns are merged by XOR
+    convolution, and equal firing probabilities share one skip table: the
+    draw must still follow the model's exact parity probabilities (computed
+    from the unmerged channels)."""
+    rng = np.random.default_rng(31)
+    num_f = 12
+    sigs = [rng.integers(0, 2, size=(num_f, 2)).astype(np.uint8) for _ in range(15)]
+    probs, cols = [], []
+    for i in range(240):                       # 16 copies of each signature pair
+        probs.append(np.array([1 - 3e-2, 1e-2, 1e-2, 1e-2]))
+        cols.append(sigs[i % 15])
+    for i in range(40):                        # one-bit channels, some never-firing
+        probs.append(np.array([1.0, 0.0]) if i % 7 == 0 else np.array([0.98, 0.02]))
+        cols.append(rng.integers(0, 2, size=(num_f, 1)).astype(np.uint8))
+    T = np.hstack(cols)
+    n = 200_000
+    f = oracle_port.noise_sample(probs, T, n, 0, 777)
+    sets = [[j] for j in range(num_f)] + [[0, 3], [1, 5, 7], [2, 4, 6, 8]]
+    for s in sets:
+        p = parity_probability(probs, T, s)
+        assert _within(float((f[:, s].sum(axis=1) % 2).mean()), p, n), (s, p)
