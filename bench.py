@@ -65,12 +65,12 @@ L2_FLUSH_BYTES = 256 << 20
 # k_sample on the same workload at 262,144 shots (dram__bytes_read.sum +
 # dram__bytes_write.sum), plus the output row the capture's L2 absorbed;
 # scaled to a launch by its shots.  Source: profiles/k_sample_cfg2_current.md.
-NCU_DRAM_BYTES_PER_SHOT = {"cfg2-medium-40q-t12": 66.2 + 40.0}
+NCU_DRAM_BYTES_PER_SHOT = {"cfg2-medium-40q-t12": 67.6 + 40.0, "cfg4-large-rank-85q-t20": 61.2 + 16.0}
 # Thread instructions per shot of the plain kernel on the same workload, from
 # one ncu capture (smsp__thread_inst_executed.sum / shots of the captured
 # launch); the issue roofline of the bench line is this times shots/s over
 # the SMs' issue ceiling.  Source: profiles/k_sample_cfg2_current.md.
-NCU_THREAD_INST_PER_SHOT = {}
+NCU_THREAD_INST_PER_SHOT = {"cfg2-medium-40q-t12": 155375, "cfg4-large-rank-85q-t20": 227680}
 # Gate locations of the workloads' circuits (qubits x depth): one
 # single-qubit Pauli channel each in the noisy end-to-end leg.
 NOISE_LOCATIONS = {"cfg2-medium-40q-t12": 40 * 200, "cfg4-large-rank-85q-t20": 85 * 600}
@@ -391,7 +391,16 @@ def plain_leg(args, torch, dev, flush, cfg):
             "ops_per_shot": work["ops"],
             "ops_per_shot_reference_model": perfmodel.reference_op_model(w.program),
             "parity": {"device_output": dev_par, "e2e_output": e2e_par},
+            "issue_frac": (NCU_THREAD_INST_PER_SHOT[w.name] * shots / (ms / 1e3) / issue_ceiling(torch, dev)
+                           if w.name in NCU_THREAD_INST_PER_SHOT else None),
             "gpu_launches": steps * len(w.program.components)}
+
+
+def issue_ceiling(torch, dev, sm_mhz=None):
+    """Thread instructions per second the SMs can issue: every sub-partition
+    issues one warp instruction a clock (4 per SM, 32 lanes)."""
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    return sms * 4 * 32 * (sm_mhz or 1965.0) * 1e6
 
 
 def bench_batched(args, torch, dev, flush):

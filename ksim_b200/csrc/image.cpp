@@ -134,7 +134,7 @@ double term_work(int W, uint32_t flags, const int n_cls[4], int n_hp, int n_pp, 
     const double c = (flags & TF_NARROW) ? 1.0 : 2.0;
     const double cn = (flags & (TF_NARROW | TF_HYBRID)) ? 1.0 : 2.0;  // NodePhases words
     double w = (double)sum_iter + 23.0 * nb;
-    if (n_cls[1] | n_cls[3]) w += 16.0 * cn + 2.0;
+    if (n_cls[1] | n_cls[3]) w += 2.0;  // the block's product read from the term's lambda table
     w += 4.0 * cn;
     w += ((n_ph + 1) / 2) * (3.0 + 5.0 + 8.0 + 8.0 + 16.0 * c + 4.0 * c + 1.0);
     w += 4.0 + (c == 1.0 ? 16.0 : 64.0) + 6.0 * c + 16.0;
@@ -641,6 +641,22 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 while (body.size() & 15u) body.push_back(0);
                 body.insert(body.end(), pair_tab.begin(), pair_tab.end());
                 body.insert(body.end(), pair_step.begin(), pair_step.end());
+                // NodePhases with class-1 / class-3 columns: C lambda^e for
+                // e = -n1 .. n3 (mod 2^64; the low words on the 32-bit
+                // NodePhases paths), so a shot reads its block's product by
+                // its lambda count instead of multiplying
+                if (n_cls[1] | n_cls[3]) {
+                    const bool np32 = (flags & (TF_NARROW | TF_HYBRID)) != 0;
+                    const Zu c = {(uint64_t)C[0], (uint64_t)C[1], (uint64_t)C[2], (uint64_t)C[3]};
+                    for (int e = -n_cls[1]; e <= n_cls[3]; ++e) {
+                        const Zu z = zmul(c, lam_pow(e, uint64_t()));
+                        const uint64_t w4[4] = {z.a, z.b, z.c, z.d};
+                        for (int k = 0; k < 4; ++k) {
+                            if (np32) put32(body, (uint32_t)w4[k]);
+                            else put64(body, w4[k]);
+                        }
+                    }
+                }
                 while (body.size() & 15u) body.push_back(0);
                 nb = (uint32_t)((rows.size() + 31) / 32);
                 const uint16_t zero_off = (uint16_t)(8 * 64 * W);

@@ -439,7 +439,41 @@ KS_HD int term_pair_tab_off(const TermHdr &h)
     return term_meta_off(h) + TERM_FFK_BYTES + ((2 * (int)h.n_cls[0] + 15) & ~15);
 }
 KS_HD int term_pair_step_off(const TermHdr &h) { return term_pair_tab_off(h) + 64 * (int)term_ph_pairs(h); }
-KS_HD int term_blocks_off(const TermHdr &h) { return term_pair_step_off(h) + 256 * (int)term_ph_pairs(h); }
+// NodePhases products C lambda^e, e = -n1 .. n3, for terms with class-1 or
+// class-3 columns (n_cls[2], n_cls[3] in run order): 4 x u32 per entry on the
+// 32-bit NodePhases paths, 4 x u64 otherwise; entry i is e = i - n1.
+KS_HD bool term_np_odd(const TermHdr &h) { return (h.n_cls[2] | h.n_cls[3]) != 0; }
+KS_HD int term_npl_off(const TermHdr &h) { return term_pair_step_off(h) + 256 * (int)term_ph_pairs(h); }
+KS_HD int term_npl_bytes(const TermHdr &h)
+{
+    if (!term_np_odd(h)) return 0;
+    const int entry = (h.flags & (TF_NARROW | TF_HYBRID)) ? 16 : 32;
+    return ((int)(h.n_cls[2] + h.n_cls[3] + 1) * entry + 15) & ~15;
+}
+KS_HD int term_blocks_off(const TermHdr &h) { return term_npl_off(h) + term_npl_bytes(h); }
+
+// Entry i of a term's lambda table in the word type of its NodePhases block.
+KS_HD Zr<uint32_t> load_npl(const uint8_t *tab, uint32_t i, uint32_t)
+{
+#if defined(__CUDA_ARCH__)
+    const uint4 x = *(const uint4 *)(tab + 16 * (size_t)i);
+    return {x.x, x.y, x.z, x.w};
+#else
+    const uint32_t *q = (const uint32_t *)(tab + 16 * (size_t)i);
+    return {q[0], q[1], q[2], q[3]};
+#endif
+}
+KS_HD Zr<uint64_t> load_npl(const uint8_t *tab, uint32_t i, uint64_t)
+{
+#if defined(__CUDA_ARCH__)
+    const ulonglong2 *q = (const ulonglong2 *)(tab + 32 * (size_t)i);
+    const ulonglong2 x = q[0], y = q[1];
+    return {x.x, x.y, y.x, y.y};
+#else
+    const uint64_t *q = (const uint64_t *)(tab + 32 * (size_t)i);
+    return {q[0], q[1], q[2], q[3]};
+#endif
+}
 KS_HD void load_i32x4(const uint8_t *p, int32_t (&r)[4])
 {
 #if defined(__CUDA_ARCH__)
@@ -591,12 +625,14 @@ KS_HD const uint8_t *eval_term_rows(const uint8_t *p, const TermHdr &h, const Ro
     // HalfPi cannot fire)
     const uint64_t *cp = (const uint64_t *)(p + TERM_NPC_OFF);
     const Zr<TN> c = {(TN)cp[0], (TN)cp[1], (TN)cp[2], (TN)cp[3]};
-    const bool odd = (h.n_cls[2] | h.n_cls[3]) != 0;
+    const bool odd = term_np_odd(h);
+    const uint8_t *npl = p + term_npl_off(h);
     Zr<T> z[S];
 #pragma unroll
     for (int s = 0; s < S; ++s) {
+        // C lambda^(m3 - m1), tabulated per term: lam = m3 + (n1 - m1)
         Zr<TN> zn = c;
-        if (odd) zn = zmul(c, lam_pow((int)lam[s] - (int)h.n_cls[2], TN()));
+        if (odd) zn = load_npl(npl, lam[s], TN());
         const TN keep = (TN)0 - (TN)alive[s];
         zn.a &= keep; zn.b &= keep; zn.c &= keep; zn.d &= keep;
         if constexpr (sizeof(TN) == sizeof(T)) {
