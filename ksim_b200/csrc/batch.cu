@@ -1,20 +1,33 @@
-// batch.cu — many components / programs in one persistent, graph-captured launch.
+// batch.cu — many components / programs in one graph-captured launch of
+// persistent kernels.
 //
-// Work is cut into items (job, tile of blockDim.x shots).  Items are ordered
+// Work is cut into items (job, tile of shots).  Items are ordered
 // longest-first (cost = tile shots x term-stream bytes of the job's component)
-// and a grid of (CTAs per SM x SMs) persistent CTAs pulls them from a device
-// work counter with one atomicAdd per item, so programs with uneven term
-// counts, output counts and shot counts share the GPU with little tail.  A
-// CTA keeps one staging ring for its whole life; its running chunk count picks
-// each copy's slot and barrier phase across items of different jobs.
+// and persistent CTAs pull them from a device work counter with one
+// atomicAdd per item, so programs with uneven term counts, output counts and
+// shot counts share the GPU with little tail.  A CTA keeps one staging ring
+// for its whole life; its running chunk count picks each copy's slot and
+// barrier phase across items of different jobs.
 //
-// Jobs are dispatched on their parameter-word class at run time: one kernel
-// covers W <= 4 (every workload of the benchmark), a second W in 5..16; a
-// batch needing only one class is one launch.  The counter reset and the
-// launch(es) are captured once into a CUDA graph and replayed.
+// Items are grouped into classes by the kernel body their job needs: (W, term
+// paths) for W <= 4 — 32-bit, hybrid or general (64-bit words / exact path)
+// bodies — and one class for W in 5..16.  Each class present in a batch is
+// drained by its own persistent kernel compiled with that one body inline
+// and no out-of-line calls (a kernel that holds several bodies, or calls
+// between them, ran 6-11 % slower on the same items), with the register
+// budget of the plain kernel for that body.  The job table travels in the
+// kernels' parameter space when it fits (BATCH_PARAM_JOBS jobs), so job fields
+// are read from the constant bank as in the plain kernel, otherwise from
+// global memory.  The class kernels are launched on forked streams (branches
+// of the captured graph) and run concurrently: the hybrid, general and wide
+// classes, which carry the heaviest items, at the highest stream priority, so
+// their CTAs are dispatched first and the 32-bit classes fill the remaining
+// and then the freed slots.  The counter reset and the launches are captured
+// once into a CUDA graph and replayed.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <memory>
 #include <numeric>
 #include <string>
@@ -38,51 +51,53 @@ struct BatchItem {
     int64_t s0;
 };
 
+// Classes: 3 (W - 1) + p for W <= 4 (p = 0 32-bit, 1 hybrid, 2 general), 12
+// for W > 4.
+constexpr int BATCH_CLASSES = 13;
+constexpr int BATCH_WIDE = 12;
+inline int batch_class(int W, int paths)
+{
+    if (W > 4) return BATCH_WIDE;
+    const int p = paths == PATHS_NARROW ? 0 : paths == PATHS_NARROW_HYBRID ? 1 : 2;
+    return 3 * (W - 1) + p;
+}
+
 namespace {
 
-// Class 0 runs W <= 4, class 1 the wider vectors; the parity scratch is
-// sized for the largest W among a launch's jobs (smaller scratch leaves more
-// of the SM's shared storage to L1).
+// The parity scratch is sized for the largest W among a class's jobs
+// (smaller scratch leaves more of the SM's shared storage to L1).
 size_t batch_smem_bytes(int slot_bytes, int max_w, int threads)
 {
     return sample_smem_bytes(slot_bytes, true, max_w, threads);
 }
 
-// One item's body per (W, term paths), each out of line: register-allocated
-// on its own, so the 32-bit and hybrid bodies keep the allocation of the
-// plain kernels compiled for those paths, and the general body (64-bit words,
-// exact path; rare) cannot raise it.  An item is a whole tile of shots, so
-// the call costs nothing measurable.
-// Shots per thread of an item: two for W <= 4 (one for the hybrid and
-// general bodies when KSIM_BATCH_WIDE_S is 1, for a smaller register budget),
-// one for wider vectors.
-#ifndef KSIM_BATCH_WIDE_S
-#define KSIM_BATCH_WIDE_S 2
-#endif
-__host__ __device__ constexpr int batch_spt(int W, int paths)
-{
-    return paths == PATHS_NARROW ? shots_per_thread(W) : (W <= 4 ? KSIM_BATCH_WIDE_S : 1);
-}
+// One launch's view of the batch: its class's items and counter, its staging
+// slot, and the job table by value (BatchParams, up to BATCH_PARAM_JOBS jobs)
+// or through a pointer (BatchParamsG).
+constexpr int BATCH_PARAM_JOBS = 180;
+struct BatchParams {
+    const BatchItem *items;
+    int *counter;
+    int32_t n_items, slot_bytes;
+    BatchJobDev jobs[BATCH_PARAM_JOBS];
+    __device__ __forceinline__ const BatchJobDev &job(int i) const { return jobs[i]; }
+};
+static_assert(sizeof(BatchParams) <= 32764, "kernel parameters are limited to 32,764 bytes");
+struct BatchParamsG {
+    const BatchItem *items;
+    int *counter;
+    int32_t n_items, slot_bytes;
+    const BatchJobDev *gjobs;
+    __device__ __forceinline__ const BatchJobDev &job(int i) const { return gjobs[i]; }
+};
 
-template <int W, int PATHS>
-__device__ __noinline__ bool batch_tile(const SampleJob &j, int64_t s0, uint64_t *bar, uint8_t *slots, uint32_t &g,
-                                        uint8_t *scratch)
-{
-    return sample_tile<W, true, false, batch_spt(W, PATHS), PATHS>(j, s0, bar, slots, g, scratch);
-}
+// Register budgets: those of the plain kernels for the 32-bit and hybrid
+// bodies (96), two CTAs of 256 for the general body (128).
+#define KSIM_BATCH_BOUNDS(P) __maxnreg__((P) == PATHS_ALL ? 128 : 96)
 
-// Class 0 (W <= 4): 128 registers, two CTAs of 256 threads per SM: on the
-// mixed benchmark batch (32-bit, hybrid and general bodies in one launch) the
-// fastest of the measured shapes (96 registers with five CTAs of 128, or with
-// one shot per thread for the hybrid bodies, ran 10-20 % slower); class 1
-// (W 5..16): the general body at up to 255.
-#ifndef KSIM_BATCH_MAXNREG
-#define KSIM_BATCH_MAXNREG 128
-#endif
-#define KSIM_BATCH_BOUNDS(C) __maxnreg__((C) == 0 ? KSIM_BATCH_MAXNREG : 255)
-template <int CLASS>
-__global__ void KSIM_BATCH_BOUNDS(CLASS) k_batch(const BatchJobDev *__restrict__ jobs,
-                                                 const BatchItem *__restrict__ items, int n_items, int *counter)
+// A class with W <= 4: one body, inline.
+template <typename PT, int W, int PATHS>
+__global__ void KSIM_BATCH_BOUNDS(PATHS) k_batch_c(const __grid_constant__ PT P)
 {
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ int s_item;
@@ -90,42 +105,64 @@ __global__ void KSIM_BATCH_BOUNDS(CLASS) k_batch(const BatchJobDev *__restrict__
     uint8_t *slots = smem + BAR_BYTES;
     ring_init(bar);
     uint32_t g = 0;
-    uint8_t *scratch = slots + (size_t)NSLOT * jobs[0].j.slot_bytes;
+    uint8_t *scratch = slots + (size_t)NSLOT * P.slot_bytes;
     for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        if (threadIdx.x == 0) s_item = atomicAdd(P.counter, 1);
         __syncthreads();
         const int it = s_item;
         __syncthreads();
-        if (it >= n_items) break;
-        const BatchItem w = items[it];
-        const BatchJobDev &J = jobs[w.job];
-        bool ok = true;
-        if (CLASS == 0) {
-            // each job takes the body compiled for the term paths it uses
-#define KSIM_BATCH_W(WW)                                                                              \
-    case WW:                                                                                          \
-        ok = J.paths == PATHS_NARROW ? batch_tile<WW, PATHS_NARROW>(J.j, w.s0, bar, slots, g, scratch) \
-             : J.paths == PATHS_NARROW_HYBRID                                                         \
-                 ? batch_tile<WW, PATHS_NARROW_HYBRID>(J.j, w.s0, bar, slots, g, scratch)            \
-                 : batch_tile<WW, PATHS_ALL>(J.j, w.s0, bar, slots, g, scratch);                     \
-        break;
-            switch (J.W) {
-            KSIM_BATCH_W(1) KSIM_BATCH_W(2) KSIM_BATCH_W(3)
-            default: KSIM_BATCH_W(4)
-            }
-#undef KSIM_BATCH_W
-        } else {
-            switch (J.W) {
-            case 5: ok = sample_tile<5, true, false, shots_per_thread(5)>(J.j, w.s0, bar, slots, g, scratch); break;
-            case 6: ok = sample_tile<6, true, false, shots_per_thread(6)>(J.j, w.s0, bar, slots, g, scratch); break;
-            case 8: ok = sample_tile<8, true, false, shots_per_thread(8)>(J.j, w.s0, bar, slots, g, scratch); break;
-            case 10: ok = sample_tile<10, true, false, shots_per_thread(10)>(J.j, w.s0, bar, slots, g, scratch); break;
-            case 12: ok = sample_tile<12, true, false, shots_per_thread(12)>(J.j, w.s0, bar, slots, g, scratch); break;
-            default: ok = sample_tile<16, true, false, shots_per_thread(16)>(J.j, w.s0, bar, slots, g, scratch); break;
-            }
+        if (it >= P.n_items) break;
+        const BatchItem w = P.items[it];
+        if (!sample_tile<W, true, false, shots_per_thread(W), PATHS>(P.job(w.job).j, w.s0, bar, slots, g, scratch))
+            break;
+    }
+}
+
+// The class with W in 5..16 (rare): the general body per W.
+template <typename PT>
+__global__ void __maxnreg__(255) k_batch_wide(const __grid_constant__ PT P)
+{
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ int s_item;
+    uint64_t *bar = (uint64_t *)smem;
+    uint8_t *slots = smem + BAR_BYTES;
+    ring_init(bar);
+    uint32_t g = 0;
+    uint8_t *scratch = slots + (size_t)NSLOT * P.slot_bytes;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(P.counter, 1);
+        __syncthreads();
+        const int it = s_item;
+        __syncthreads();
+        if (it >= P.n_items) break;
+        const BatchItem w = P.items[it];
+        const BatchJobDev &J = P.job(w.job);
+        bool ok;
+        switch (J.W) {
+        case 5: ok = sample_tile<5, true, false, shots_per_thread(5)>(J.j, w.s0, bar, slots, g, scratch); break;
+        case 6: ok = sample_tile<6, true, false, shots_per_thread(6)>(J.j, w.s0, bar, slots, g, scratch); break;
+        case 8: ok = sample_tile<8, true, false, shots_per_thread(8)>(J.j, w.s0, bar, slots, g, scratch); break;
+        case 10: ok = sample_tile<10, true, false, shots_per_thread(10)>(J.j, w.s0, bar, slots, g, scratch); break;
+        case 12: ok = sample_tile<12, true, false, shots_per_thread(12)>(J.j, w.s0, bar, slots, g, scratch); break;
+        default: ok = sample_tile<16, true, false, shots_per_thread(16)>(J.j, w.s0, bar, slots, g, scratch); break;
         }
         if (!ok) break;
     }
+}
+
+// The kernel of class `cls` for job-table type PT.
+template <typename PT>
+const void *batch_kernel(int cls)
+{
+#define KSIM_BK(WW)                                                                  \
+    case 3 * (WW - 1): return (const void *)k_batch_c<PT, WW, PATHS_NARROW>;         \
+    case 3 * (WW - 1) + 1: return (const void *)k_batch_c<PT, WW, PATHS_NARROW_HYBRID>; \
+    case 3 * (WW - 1) + 2: return (const void *)k_batch_c<PT, WW, PATHS_ALL>;
+    switch (cls) {
+    KSIM_BK(1) KSIM_BK(2) KSIM_BK(3) KSIM_BK(4)
+    default: return (const void *)k_batch_wide<PT>;
+    }
+#undef KSIM_BK
 }
 
 }  // namespace
@@ -134,37 +171,90 @@ __global__ void KSIM_BATCH_BOUNDS(CLASS) k_batch(const BatchJobDev *__restrict__
 
 using namespace ksim;
 
+namespace {
+
+// One class of a batch: launch shape, items, and its stream branch.
+struct BatchClass {
+    int threads = 128, slot = 12288, max_w = 1;
+    size_t smem = 0;
+    BatchItem *d_items = nullptr;
+    int n_items = 0, grid = 0;
+    bool high = false;  // hybrid, general and wide classes: highest stream priority
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+    std::unique_ptr<BatchParams> p;  // the job table by value (<= BATCH_PARAM_JOBS jobs)
+    BatchParamsG pg = {};            // otherwise through a pointer
+};
+
+}  // namespace
+
 struct ksim_batch {
     int device = 0;
-    int threads = 256, slot_bytes = 16384, ctas_per_sm = 0, use_graph = 1;
-    int max_w[2] = {1, 5};  // largest W among each class's jobs (parity scratch size)
+    int threads = 128, slot_bytes = 12288, ctas_per_sm = 0, use_graph = 1;  // 32-bit classes (tuned)
+    BatchClass cls[BATCH_CLASSES];
     std::vector<ksim_component *> comps;
     std::vector<BatchJobDev> host_jobs;
     BatchJobDev *d_jobs = nullptr;
-    BatchItem *d_items[2] = {nullptr, nullptr};
-    int n_items[2] = {0, 0};
-    int grid[2] = {0, 0};
     int *d_counter = nullptr;
+    int prio_hi = 0, prio_lo = 0;
     cudaStream_t cap_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 };
 
+// Drop the captured graph (its kernel nodes hold the job table by value).
+static void batch_drop_graph(ksim_batch *b)
+{
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+}
+
+static cudaError_t batch_launch_class(ksim_batch *b, int c, cudaStream_t st)
+{
+    BatchClass &k = b->cls[c];
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3((unsigned)k.grid);
+    lc.blockDim = dim3((unsigned)k.threads);
+    lc.dynamicSmemBytes = k.smem;
+    lc.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributePriority;
+    at[0].val.priority = k.high ? b->prio_hi : b->prio_lo;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    if (k.p) {
+        void *args[] = {(void *)k.p.get()};
+        return cudaLaunchKernelExC(&lc, batch_kernel<BatchParams>(c), args);
+    }
+    void *args[] = {(void *)&k.pg};
+    return cudaLaunchKernelExC(&lc, batch_kernel<BatchParamsG>(c), args);
+}
+
 static ksim_status batch_enqueue(ksim_batch *b, cudaStream_t st)
 {
-    cudaError_t e = cudaMemsetAsync(b->d_counter, 0, 2 * sizeof(int), st);
+    cudaError_t e = cudaMemsetAsync(b->d_counter, 0, BATCH_CLASSES * sizeof(int), st);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(work counter)");
-    for (int cls = 0; cls < 2; ++cls) {
-        if (!b->n_items[cls]) continue;
-        const size_t smem = batch_smem_bytes(b->slot_bytes, b->max_w[cls], b->threads);
-        if (cls == 0)
-            k_batch<0><<<b->grid[0], b->threads, smem, st>>>(b->d_jobs, b->d_items[0], b->n_items[0], b->d_counter);
-        else
-            k_batch<1><<<b->grid[1], b->threads, smem, st>>>(b->d_jobs, b->d_items[1], b->n_items[1],
-                                                             b->d_counter + 1);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return cuda_fail(e, "batch kernel launch");
+    // the high-priority classes first
+    std::vector<int> active;
+    for (int pass = 0; pass < 2; ++pass)
+        for (int c = 0; c < BATCH_CLASSES; ++c)
+            if (b->cls[c].n_items && b->cls[c].high == (pass == 0)) active.push_back(c);
+    if (active.size() == 1) {
+        e = batch_launch_class(b, active[0], st);
+        return e == cudaSuccess ? KSIM_OK : cuda_fail(e, "batch kernel launch");
     }
+    if (!active.empty() && (e = cudaEventRecord(b->ev_fork, st)) != cudaSuccess) return cuda_fail(e, "batch fork");
+    for (int c : active) {
+        BatchClass &k = b->cls[c];
+        if ((e = cudaStreamWaitEvent(k.st, b->ev_fork, 0)) != cudaSuccess) return cuda_fail(e, "batch fork");
+        if ((e = batch_launch_class(b, c, k.st)) != cudaSuccess) return cuda_fail(e, "batch kernel launch");
+        if ((e = cudaEventRecord(k.done, k.st)) != cudaSuccess) return cuda_fail(e, "batch join");
+    }
+    for (int c : active)
+        if ((e = cudaStreamWaitEvent(st, b->cls[c].done, 0)) != cudaSuccess) return cuda_fail(e, "batch join");
     return KSIM_OK;
 }
 
@@ -177,6 +267,7 @@ ksim_status ksim_batch_create(const ksim_batch_job *jobs, int32_t n_jobs, const 
     *out = nullptr;
     if (n_jobs <= 0 || !jobs) return fail(KSIM_ERR_INVALID_ARGUMENT, "a batch needs at least one job");
     std::unique_ptr<ksim_batch> b(new ksim_batch());
+    const bool slot_given = tuning && tuning->slot_bytes > 0;
     if (tuning) {
         if (tuning->threads > 0) b->threads = tuning->threads;
         if (tuning->slot_bytes > 0) b->slot_bytes = tuning->slot_bytes;
@@ -188,6 +279,17 @@ ksim_status ksim_batch_create(const ksim_batch_job *jobs, int32_t n_jobs, const 
     if ((b->slot_bytes & 15) || batch_smem_bytes(b->slot_bytes, 4, b->threads) > 227 * 1024)
         return fail(KSIM_ERR_INVALID_ARGUMENT,
                     "slot_bytes must be a multiple of 16, and two slots with the parity scratch fit in 227 KiB");
+    // shapes: the 32-bit classes the tuned one; hybrid CTAs of 128 (the plain
+    // hybrid kernel's), general and wide CTAs of 256; slots at least the tuned
+    // size (16 KiB for general and wide) and every job's largest term
+    for (int c = 0; c < BATCH_CLASSES; ++c) {
+        BatchClass &k = b->cls[c];
+        const int p = c == BATCH_WIDE ? 3 : c % 3;
+        k.threads = p == 0 ? b->threads : p == 1 ? 128 : 256;
+        k.slot = p >= 2 ? std::max(16384, b->slot_bytes) : b->slot_bytes;
+        k.high = p != 0;
+        k.max_w = c == BATCH_WIDE ? 5 : c / 3 + 1;
+    }
     int device = -1;
     for (int i = 0; i < n_jobs; ++i) {
         const ksim_batch_job &jb = jobs[i];
@@ -202,24 +304,37 @@ ksim_status ksim_batch_create(const ksim_batch_job *jobs, int32_t n_jobs, const 
             return fail(KSIM_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": bad rng_mode");
         if (jb.B > 0 && ((c->img.F > 0 && !jb.d_f) || (c->img.n_out > 0 && !jb.d_out)))
             return fail(KSIM_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": NULL buffer");
-        if (c->img.max_term_bytes > b->slot_bytes)
+        if (!jb.d_out_cols && jb.out_stride < jb.out_col0 + c->img.n_out)
+            return fail(KSIM_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": out_stride too small");
+        const int cl = batch_class(c->img.W, c->cfg.paths);
+        BatchClass &k = b->cls[cl];
+        const int64_t need = (c->img.max_term_bytes + 15) & ~int64_t(15);
+        // a slot the caller chose must hold the 32-bit jobs' terms; the
+        // default and the other classes' slots grow to their largest term
+        if (slot_given && cl % 3 == 0 && cl != BATCH_WIDE && need > b->slot_bytes)
             return fail(KSIM_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": a term record (" +
                                                        std::to_string(c->img.max_term_bytes) +
                                                        " bytes) exceeds slot_bytes");
-        if (!jb.d_out_cols && jb.out_stride < jb.out_col0 + c->img.n_out)
-            return fail(KSIM_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": out_stride too small");
+        if (need > k.slot) k.slot = (int)std::min<int64_t>(need, 1 << 30);
+        k.max_w = std::max(k.max_w, c->img.W);
     }
+    for (int c = 0; c < BATCH_CLASSES; ++c)
+        if (batch_smem_bytes(b->cls[c].slot, b->cls[c].max_w, b->cls[c].threads) > 227 * 1024)
+            return fail(KSIM_ERR_UNSUPPORTED, "a term record needs a staging slot of " +
+                                                  std::to_string(b->cls[c].slot) + " bytes, beyond shared memory");
     b->device = device;
     DeviceGuard g(device);
-    LaunchCfg cfg;
-    cfg.threads = b->threads;
-    cfg.staged = 1;
-    cfg.slot_bytes = b->slot_bytes;
-    std::vector<BatchItem> items[2];
-    std::vector<double> cost[2];
+    std::vector<BatchItem> items[BATCH_CLASSES];
+    std::vector<double> cost[BATCH_CLASSES];
     for (int i = 0; i < n_jobs; ++i) {
         const ksim_batch_job &jb = jobs[i];
         ksim_component *c = jb.comp;
+        const int cl = batch_class(c->img.W, c->cfg.paths);
+        BatchClass &k = b->cls[cl];
+        LaunchCfg cfg;
+        cfg.threads = k.threads;
+        cfg.staged = 1;
+        cfg.slot_bytes = k.slot;
         BatchJobDev d = {};
         ksim_status st = component_job(c, cfg, d.j);
         if (st != KSIM_OK) return st;
@@ -242,53 +357,74 @@ ksim_status ksim_batch_create(const ksim_batch_job *jobs, int32_t n_jobs, const 
         if (c->img.n_out == 0 || jb.B == 0) continue;
         double bytes = 0;
         for (const GraphDir &gd : c->img.gdir) bytes += (double)gd.stream_bytes + 64.0;
-        const int cls = d.W <= 4 ? 0 : 1;
-        b->max_w[cls] = std::max(b->max_w[cls], d.W);
-        const int64_t tile = (int64_t)b->threads * batch_spt(d.W, d.paths);
+        const int64_t tile = (int64_t)k.threads * shots_per_thread(d.W);
         for (int64_t s0 = 0; s0 < jb.B; s0 += tile) {
             BatchItem it = {};
             it.job = i;
             it.s0 = s0;
-            items[cls].push_back(it);
-            cost[cls].push_back(bytes * (double)std::min<int64_t>(tile, jb.B - s0));
+            items[cl].push_back(it);
+            cost[cl].push_back(bytes * (double)std::min<int64_t>(tile, jb.B - s0));
         }
     }
     cudaError_t e = cudaMalloc(&b->d_jobs, sizeof(BatchJobDev) * b->host_jobs.size());
     if (e == cudaSuccess)
         e = cudaMemcpy(b->d_jobs, b->host_jobs.data(), sizeof(BatchJobDev) * b->host_jobs.size(),
                        cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_counter, 2 * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_counter, BATCH_CLASSES * sizeof(int));
+    if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&b->prio_lo, &b->prio_hi);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         ksim_batch_destroy(b.release());
         return cuda_fail(e, "batch upload");
     }
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    for (int cls = 0; cls < 2; ++cls) {
-        const size_t smem = batch_smem_bytes(b->slot_bytes, b->max_w[cls], b->threads);
-        std::vector<int> order(items[cls].size());
+    const bool by_value = b->host_jobs.size() <= (size_t)BATCH_PARAM_JOBS;
+    for (int c = 0; c < BATCH_CLASSES; ++c) {
+        BatchClass &k = b->cls[c];
+        if (items[c].empty()) continue;
+        k.smem = batch_smem_bytes(k.slot, k.max_w, k.threads);
+        std::vector<int> order(items[c].size());
         std::iota(order.begin(), order.end(), 0);
-        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[cls][x] > cost[cls][y]; });
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[c][x] > cost[c][y]; });
         std::vector<BatchItem> sorted;
         sorted.reserve(order.size());
-        for (int o : order) sorted.push_back(items[cls][o]);
-        b->n_items[cls] = (int)sorted.size();
-        if (sorted.empty()) continue;
-        e = cudaMalloc(&b->d_items[cls], sizeof(BatchItem) * sorted.size());
+        for (int o : order) sorted.push_back(items[c][o]);
+        k.n_items = (int)sorted.size();
+        e = cudaMalloc(&k.d_items, sizeof(BatchItem) * sorted.size());
         if (e == cudaSuccess)
-            e = cudaMemcpy(b->d_items[cls], sorted.data(), sizeof(BatchItem) * sorted.size(), cudaMemcpyHostToDevice);
+            e = cudaMemcpy(k.d_items, sorted.data(), sizeof(BatchItem) * sorted.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&k.st, cudaStreamNonBlocking, k.high ? b->prio_hi : b->prio_lo);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&k.done, cudaEventDisableTiming);
+        if (by_value) {
+            k.p.reset(new BatchParams());
+            std::memset(k.p.get(), 0, sizeof(BatchParams));
+            k.p->items = k.d_items;
+            k.p->counter = b->d_counter + c;
+            k.p->n_items = k.n_items;
+            k.p->slot_bytes = k.slot;
+            std::copy(b->host_jobs.begin(), b->host_jobs.end(), k.p->jobs);
+        } else {
+            k.pg.items = k.d_items;
+            k.pg.counter = b->d_counter + c;
+            k.pg.n_items = k.n_items;
+            k.pg.slot_bytes = k.slot;
+            k.pg.gjobs = b->d_jobs;
+        }
         int active = 0;
         if (e == cudaSuccess) {
-            const void *fn = cls == 0 ? (const void *)k_batch<0> : (const void *)k_batch<1>;
-            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&active, fn, b->threads, smem);
+            const void *fn = by_value ? batch_kernel<BatchParams>(c) : batch_kernel<BatchParamsG>(c);
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
+            if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&active, fn, k.threads, k.smem);
         }
         if (e != cudaSuccess) {
             ksim_batch_destroy(b.release());
             return cuda_fail(e, "batch setup");
         }
-        const int per_sm = b->ctas_per_sm > 0 ? std::min(b->ctas_per_sm, std::max(active, 1)) : std::max(active, 1);
-        b->grid[cls] = std::max(1, std::min(per_sm * sms, b->n_items[cls]));
+        const int per_sm = (c % 3 == 0 && c != BATCH_WIDE && b->ctas_per_sm > 0)
+                               ? std::min(b->ctas_per_sm, std::max(active, 1))
+                               : std::max(active, 1);
+        k.grid = std::max(1, std::min(per_sm * sms, k.n_items));
     }
     *out = b.release();
     return KSIM_OK;
@@ -302,6 +438,13 @@ ksim_status ksim_batch_set_seeds(ksim_batch *b, const uint64_t *seeds)
     cudaError_t e = cudaMemcpy(b->d_jobs, b->host_jobs.data(), sizeof(BatchJobDev) * b->host_jobs.size(),
                                cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_fail(e, "batch seeds");
+    bool by_value = false;
+    for (BatchClass &k : b->cls)
+        if (k.p) {
+            by_value = true;
+            for (size_t i = 0; i < b->host_jobs.size(); ++i) k.p->jobs[i].j.seed = seeds[i];
+        }
+    if (by_value) batch_drop_graph(b);  // recaptured with the new seeds on the next launch
     return KSIM_OK;
 }
 
@@ -312,7 +455,8 @@ ksim_status ksim_batch_launch(ksim_batch *b, void *stream)
     cudaStream_t st = (cudaStream_t)stream;
     if (!b->use_graph) return batch_enqueue(b, st);
     if (!b->exec) {
-        cudaError_t e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
+        cudaError_t e = cudaSuccess;
+        if (!b->cap_stream) e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
         e = cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
@@ -331,9 +475,17 @@ ksim_status ksim_batch_launch(ksim_batch *b, void *stream)
 ksim_status ksim_batch_info(const ksim_batch *b, int64_t *n_items, int32_t *grid, int32_t *n_launches)
 {
     if (!b) return fail(KSIM_ERR_INVALID_ARGUMENT, "batch is NULL");
-    if (n_items) *n_items = (int64_t)b->n_items[0] + b->n_items[1];
-    if (grid) *grid = b->grid[0] + b->grid[1];
-    if (n_launches) *n_launches = (b->n_items[0] ? 1 : 0) + (b->n_items[1] ? 1 : 0);
+    int64_t n = 0;
+    int32_t gsum = 0, l = 0;
+    for (const BatchClass &k : b->cls)
+        if (k.n_items) {
+            n += k.n_items;
+            gsum += k.grid;
+            ++l;
+        }
+    if (n_items) *n_items = n;
+    if (grid) *grid = gsum;
+    if (n_launches) *n_launches = l;
     return KSIM_OK;
 }
 
@@ -342,11 +494,14 @@ void ksim_batch_destroy(ksim_batch *b)
     if (!b) return;
     DeviceGuard g(b->device);
     cudaDeviceSynchronize();
-    if (b->exec) cudaGraphExecDestroy(b->exec);
-    if (b->graph) cudaGraphDestroy(b->graph);
+    batch_drop_graph(b);
     if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
-    for (int c = 0; c < 2; ++c)
-        if (b->d_items[c]) cudaFree(b->d_items[c]);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    for (BatchClass &k : b->cls) {
+        if (k.st) cudaStreamDestroy(k.st);
+        if (k.done) cudaEventDestroy(k.done);
+        if (k.d_items) cudaFree(k.d_items);
+    }
     if (b->d_jobs) cudaFree(b->d_jobs);
     if (b->d_counter) cudaFree(b->d_counter);
     delete b;

@@ -44,6 +44,25 @@ def mixed():
     return _mixed_programs()
 
 
+def _classes(progs, shots):
+    """(W class, term-path class) of every component with work: W above 4 is
+    one class, below it each W with 32-bit / hybrid / general terms."""
+    from ksim_b200 import perfmodel
+    from ksim_b200.kokkos_sim import Component
+    out = set()
+    for prog, b in zip(progs, shots):
+        for comp in prog.components:
+            if b == 0 or len(comp.graphs) <= 1:
+                continue
+            w = Component(comp.graphs, int(np.asarray(comp.f_selection).shape[0])).words
+            r = perfmodel.component_work(comp)
+            terms = r["narrow_terms"] + r["wide_terms"] + r["exact_terms"] + r["hybrid_terms"]
+            paths = (0 if r["narrow_terms"] == terms else
+                     1 if r["narrow_terms"] + r["hybrid_terms"] == terms else 2)
+            out.add((w, paths) if w <= 4 else ("wide",))
+    return out
+
+
 def _oracle(oracle_port, progs, fs, seeds, mode):
     return [oracle_port.program_sample(p, f, s, rng_mode=mode) for p, f, s in zip(progs, fs, seeds)]
 
@@ -54,7 +73,8 @@ def test_batch_matches_oracle(cuda_device, oracle_port, mixed, mode):
     progs, shots, fs = mixed
     seeds = [17 + 1000 * i for i in range(len(progs))]
     bs = BatchSampler(progs, shots, seeds=seeds, rng_mode=mode, n_f=[f.shape[1] for f in fs])
-    assert bs.info()["launches"] == 2  # one W-class kernel per class present
+    # one persistent kernel per (W, term paths) class with work
+    assert bs.info()["launches"] == len(_classes(progs, shots))
     got = bs.sample(fs)
     want = _oracle(oracle_port, progs, fs, seeds, mode)
     for i, (g, w) in enumerate(zip(got, want)):
