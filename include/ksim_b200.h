@@ -294,12 +294,12 @@ typedef struct ksim_batch_job {
 } ksim_batch_job;
 
 /* Launch shape of a batch (zero / negative fields take the defaults:
- * 128 threads, 12 KiB slots, CTAs per SM from occupancy, graph on).  The
+ * 128 threads, 14 KiB slots, CTAs per SM from occupancy, graph on).  The
  * shape applies to the jobs whose terms all run on 32-bit words with W <= 4
  * (the bulk of the work), drained by one persistent kernel; jobs with hybrid,
  * 64-bit or exact-path terms and jobs with W > 4 run in kernels of their own
- * (CTAs of 256, slots of at least 16 KiB), concurrently with it and at a
- * higher stream priority.  A work item is 2 x threads shots of a W <= 4 job
+ * (CTAs of 128; slots of at least 16 KiB for 64-bit, exact and W > 4 terms),
+ * launched before it and overlapping it.  A work item is 2 x threads shots of a W <= 4 job
  * (two shots per thread) and threads shots of a wider one. */
 typedef struct ksim_batch_tuning {
     int32_t threads;      /* threads per CTA (a multiple of 32, <= 256); see the item size above */

@@ -31,10 +31,10 @@ from .sampler import B200ProgramSampler
 
 __all__ = ["BatchSampler", "tune_cache_path"]
 
-_DEFAULT_TUNING = {"threads": 128, "slot_bytes": 12288, "ctas_per_sm": 0}
+_DEFAULT_TUNING = {"threads": 128, "slot_bytes": 14336, "ctas_per_sm": 0}
 _CANDIDATES = [
     {"threads": t, "slot_bytes": s, "ctas_per_sm": c}
-    for t in (64, 128, 256) for s in (8192, 12288, 16384) for c in (0,)
+    for t in (64, 128, 256) for s in (8192, 12288, 14336, 16384) for c in (0, 4)
 ]
 
 

@@ -18,12 +18,13 @@
 // budget of the plain kernel for that body.  The job table travels in the
 // kernels' parameter space when it fits (BATCH_PARAM_JOBS jobs), so job fields
 // are read from the constant bank as in the plain kernel, otherwise from
-// global memory.  The class kernels are launched on forked streams (branches
-// of the captured graph) and run concurrently: the hybrid, general and wide
-// classes, which carry the heaviest items, at the highest stream priority, so
-// their CTAs are dispatched first and the 32-bit classes fill the remaining
-// and then the freed slots.  The counter reset and the launches are captured
-// once into a CUDA graph and replayed.
+// global memory.  The class kernels go on one stream in a fixed order — the
+// hybrid, general and wide classes (the heaviest items) first, then the
+// 32-bit ones, each group by its costliest item — as programmatic dependent
+// launches: each kernel starts once every CTA of the one before it runs, and
+// fills the slots that one frees as it drains, so the classes overlap without
+// the run-to-run dispatch order of concurrent graph branches.  The counter
+// reset and the launches are captured once into a CUDA graph and replayed.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -91,9 +92,33 @@ struct BatchParamsG {
     __device__ __forceinline__ const BatchJobDev &job(int i) const { return gjobs[i]; }
 };
 
+// CTA sizes of the hybrid and of the general / wide classes.  Their items
+// are the heaviest (up to a few times a 32-bit item's work per shot), and a
+// smaller CTA is a shorter item, so the last ones end sooner; these jobs also
+// tend to have few shots, and 128-thread CTAs spread them over four times the
+// SMs of 256-thread ones (a 57-qubit, 11,170-shot general job: 1.78 against
+// 2.22 ms alone on the GPU).
+#ifndef KSIM_BATCH_HYB_THREADS
+#define KSIM_BATCH_HYB_THREADS 128
+#endif
+#ifndef KSIM_BATCH_GEN_THREADS
+#define KSIM_BATCH_GEN_THREADS 128
+#endif
+
 // Register budgets: those of the plain kernels for the 32-bit and hybrid
-// bodies (96), two CTAs of 256 for the general body (128).
+// bodies (96), four CTAs of 128 for the general body (128).
 #define KSIM_BATCH_BOUNDS(P) __maxnreg__((P) == PATHS_ALL ? 128 : 96)
+
+// Programmatic dependent launch: the class kernels are launched on one
+// stream, heaviest class first, each allowed to start once every CTA of the
+// previous one runs (launch_dependents, at a CTA's start), so they overlap and
+// a later class fills the slots the earlier ones leave; before leaving, a CTA
+// waits until the previous class's kernel has finished (wait), so the stream
+// still completes in launch order.  A kernel starts only after all CTAs of
+// its predecessor are resident, so the wait never holds slots its
+// predecessor needs.
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 // A class with W <= 4: one body, inline.
 template <typename PT, int W, int PATHS>
@@ -104,6 +129,7 @@ __global__ void KSIM_BATCH_BOUNDS(PATHS) k_batch_c(const __grid_constant__ PT P)
     uint64_t *bar = (uint64_t *)smem;
     uint8_t *slots = smem + BAR_BYTES;
     ring_init(bar);
+    pdl_launch_dependents();
     uint32_t g = 0;
     uint8_t *scratch = slots + (size_t)NSLOT * P.slot_bytes;
     for (;;) {
@@ -116,6 +142,7 @@ __global__ void KSIM_BATCH_BOUNDS(PATHS) k_batch_c(const __grid_constant__ PT P)
         if (!sample_tile<W, true, false, shots_per_thread(W), PATHS>(P.job(w.job).j, w.s0, bar, slots, g, scratch))
             break;
     }
+    pdl_wait();
 }
 
 // The class with W in 5..16 (rare): the general body per W.
@@ -127,6 +154,7 @@ __global__ void __maxnreg__(255) k_batch_wide(const __grid_constant__ PT P)
     uint64_t *bar = (uint64_t *)smem;
     uint8_t *slots = smem + BAR_BYTES;
     ring_init(bar);
+    pdl_launch_dependents();
     uint32_t g = 0;
     uint8_t *scratch = slots + (size_t)NSLOT * P.slot_bytes;
     for (;;) {
@@ -148,6 +176,7 @@ __global__ void __maxnreg__(255) k_batch_wide(const __grid_constant__ PT P)
         }
         if (!ok) break;
     }
+    pdl_wait();
 }
 
 // The kernel of class `cls` for job-table type PT.
@@ -173,15 +202,14 @@ using namespace ksim;
 
 namespace {
 
-// One class of a batch: launch shape, items, and its stream branch.
+// One class of a batch: launch shape and items.
 struct BatchClass {
-    int threads = 128, slot = 12288, max_w = 1;
+    int threads = 128, slot = 14336, max_w = 1;
     size_t smem = 0;
     BatchItem *d_items = nullptr;
     int n_items = 0, grid = 0;
-    bool high = false;  // hybrid, general and wide classes: highest stream priority
-    cudaStream_t st = nullptr;
-    cudaEvent_t done = nullptr;
+    bool high = false;      // hybrid, general and wide classes: launched before the 32-bit ones
+    double head_cost = 0;   // cost of its costliest item
     std::unique_ptr<BatchParams> p;  // the job table by value (<= BATCH_PARAM_JOBS jobs)
     BatchParamsG pg = {};            // otherwise through a pointer
 };
@@ -190,15 +218,13 @@ struct BatchClass {
 
 struct ksim_batch {
     int device = 0;
-    int threads = 128, slot_bytes = 12288, ctas_per_sm = 0, use_graph = 1;  // 32-bit classes (tuned)
+    int threads = 128, slot_bytes = 14336, ctas_per_sm = 0, use_graph = 1;  // 32-bit classes (tuned)
     BatchClass cls[BATCH_CLASSES];
     std::vector<ksim_component *> comps;
     std::vector<BatchJobDev> host_jobs;
     BatchJobDev *d_jobs = nullptr;
     int *d_counter = nullptr;
-    int prio_hi = 0, prio_lo = 0;
     cudaStream_t cap_stream = nullptr;
-    cudaEvent_t ev_fork = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 };
@@ -212,7 +238,9 @@ static void batch_drop_graph(ksim_batch *b)
     b->graph = nullptr;
 }
 
-static cudaError_t batch_launch_class(ksim_batch *b, int c, cudaStream_t st)
+// Launch class c's kernel on `st`; `follow`: it may start as soon as every CTA
+// of the kernel launched before it on `st` runs (programmatic dependent launch).
+static cudaError_t batch_launch_class(ksim_batch *b, int c, cudaStream_t st, bool follow)
 {
     BatchClass &k = b->cls[c];
     cudaLaunchConfig_t lc = {};
@@ -221,10 +249,10 @@ static cudaError_t batch_launch_class(ksim_batch *b, int c, cudaStream_t st)
     lc.dynamicSmemBytes = k.smem;
     lc.stream = st;
     cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributePriority;
-    at[0].val.priority = k.high ? b->prio_hi : b->prio_lo;
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
     lc.attrs = at;
-    lc.numAttrs = 1;
+    lc.numAttrs = follow ? 1 : 0;
     if (k.p) {
         void *args[] = {(void *)k.p.get()};
         return cudaLaunchKernelExC(&lc, batch_kernel<BatchParams>(c), args);
@@ -237,24 +265,19 @@ static ksim_status batch_enqueue(ksim_batch *b, cudaStream_t st)
 {
     cudaError_t e = cudaMemsetAsync(b->d_counter, 0, BATCH_CLASSES * sizeof(int), st);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(work counter)");
-    // the high-priority classes first
+    // the hybrid / general / wide classes first, then the 32-bit ones; within
+    // each group the class with the costliest first item first
     std::vector<int> active;
-    for (int pass = 0; pass < 2; ++pass)
-        for (int c = 0; c < BATCH_CLASSES; ++c)
-            if (b->cls[c].n_items && b->cls[c].high == (pass == 0)) active.push_back(c);
-    if (active.size() == 1) {
-        e = batch_launch_class(b, active[0], st);
-        return e == cudaSuccess ? KSIM_OK : cuda_fail(e, "batch kernel launch");
-    }
-    if (!active.empty() && (e = cudaEventRecord(b->ev_fork, st)) != cudaSuccess) return cuda_fail(e, "batch fork");
-    for (int c : active) {
-        BatchClass &k = b->cls[c];
-        if ((e = cudaStreamWaitEvent(k.st, b->ev_fork, 0)) != cudaSuccess) return cuda_fail(e, "batch fork");
-        if ((e = batch_launch_class(b, c, k.st)) != cudaSuccess) return cuda_fail(e, "batch kernel launch");
-        if ((e = cudaEventRecord(k.done, k.st)) != cudaSuccess) return cuda_fail(e, "batch join");
-    }
-    for (int c : active)
-        if ((e = cudaStreamWaitEvent(st, b->cls[c].done, 0)) != cudaSuccess) return cuda_fail(e, "batch join");
+    for (int c = 0; c < BATCH_CLASSES; ++c)
+        if (b->cls[c].n_items) active.push_back(c);
+    std::stable_sort(active.begin(), active.end(), [&](int x, int y) {
+        const BatchClass &a = b->cls[x], &z = b->cls[y];
+        if (a.high != z.high) return a.high;
+        return a.head_cost > z.head_cost;
+    });
+    for (size_t i = 0; i < active.size(); ++i)
+        if ((e = batch_launch_class(b, active[i], st, i > 0)) != cudaSuccess)
+            return cuda_fail(e, "batch kernel launch");
     return KSIM_OK;
 }
 
@@ -279,13 +302,14 @@ ksim_status ksim_batch_create(const ksim_batch_job *jobs, int32_t n_jobs, const 
     if ((b->slot_bytes & 15) || batch_smem_bytes(b->slot_bytes, 4, b->threads) > 227 * 1024)
         return fail(KSIM_ERR_INVALID_ARGUMENT,
                     "slot_bytes must be a multiple of 16, and two slots with the parity scratch fit in 227 KiB");
-    // shapes: the 32-bit classes the tuned one; hybrid CTAs of 128 (the plain
-    // hybrid kernel's), general and wide CTAs of 256; slots at least the tuned
-    // size (16 KiB for general and wide) and every job's largest term
+    // shapes: the 32-bit classes the tuned one; hybrid CTAs of
+    // KSIM_BATCH_HYB_THREADS, general and wide CTAs of KSIM_BATCH_GEN_THREADS;
+    // slots at least the tuned size (16 KiB for general and wide) and every
+    // job's largest term
     for (int c = 0; c < BATCH_CLASSES; ++c) {
         BatchClass &k = b->cls[c];
         const int p = c == BATCH_WIDE ? 3 : c % 3;
-        k.threads = p == 0 ? b->threads : p == 1 ? 128 : 256;
+        k.threads = p == 0 ? b->threads : p == 1 ? KSIM_BATCH_HYB_THREADS : KSIM_BATCH_GEN_THREADS;
         k.slot = p >= 2 ? std::max(16384, b->slot_bytes) : b->slot_bytes;
         k.high = p != 0;
         k.max_w = c == BATCH_WIDE ? 5 : c / 3 + 1;
@@ -371,8 +395,6 @@ ksim_status ksim_batch_create(const ksim_batch_job *jobs, int32_t n_jobs, const 
         e = cudaMemcpy(b->d_jobs, b->host_jobs.data(), sizeof(BatchJobDev) * b->host_jobs.size(),
                        cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_counter, BATCH_CLASSES * sizeof(int));
-    if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&b->prio_lo, &b->prio_hi);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         ksim_batch_destroy(b.release());
         return cuda_fail(e, "batch upload");
@@ -391,11 +413,10 @@ ksim_status ksim_batch_create(const ksim_batch_job *jobs, int32_t n_jobs, const 
         sorted.reserve(order.size());
         for (int o : order) sorted.push_back(items[c][o]);
         k.n_items = (int)sorted.size();
+        k.head_cost = cost[c][order[0]];
         e = cudaMalloc(&k.d_items, sizeof(BatchItem) * sorted.size());
         if (e == cudaSuccess)
             e = cudaMemcpy(k.d_items, sorted.data(), sizeof(BatchItem) * sorted.size(), cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&k.st, cudaStreamNonBlocking, k.high ? b->prio_hi : b->prio_lo);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&k.done, cudaEventDisableTiming);
         if (by_value) {
             k.p.reset(new BatchParams());
             std::memset(k.p.get(), 0, sizeof(BatchParams));
@@ -496,10 +517,7 @@ void ksim_batch_destroy(ksim_batch *b)
     cudaDeviceSynchronize();
     batch_drop_graph(b);
     if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
-    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
     for (BatchClass &k : b->cls) {
-        if (k.st) cudaStreamDestroy(k.st);
-        if (k.done) cudaEventDestroy(k.done);
         if (k.d_items) cudaFree(k.d_items);
     }
     if (b->d_jobs) cudaFree(b->d_jobs);
