@@ -79,7 +79,7 @@ NOISE_LOCATIONS = {"cfg2-medium-40q-t12": 40 * 200, "cfg4-large-rank-85q-t20": 8
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", type=int, default=2, choices=(1, 2, 4))
@@ -105,13 +105,13 @@ def parse():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons every 20 ms; summary() keeps the
+    """nvidia-smi clocks / throttle reasons every 10 ms; summary() keeps the
     samples taken inside the timed region (between begin() and end())."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index: int, period_ms: int = 20):
+    def __init__(self, index: int, period_ms: int = 10):
         self.index = index
         self.period_ms = period_ms
         self.proc = None
