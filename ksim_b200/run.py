@@ -13,8 +13,9 @@ so only the output bits cross PCIe, and the sampler is the B200 drop-in.
 
 The compile step (stim parsing, ZX reduction, stabilizer-rank decomposition:
 ``ksim.compile``) is not part of this package; ``sample_circuit`` takes it as
-a callable, e.g. the reference's ``ksim.compile_cache.compile`` bound to its
-arguments, and ``sample_compiled`` takes its result directly.
+a callable, e.g. the reference's ``ksim.compile`` (``__init__.py:75-91``:
+circuit -> (FlatProgram, channel_probs, error_transform), through its
+compile cache), and ``sample_compiled`` takes its result directly.
 
 Backends: "b200" (alias "gpu", the reference's name for its device path) and
 "auto" (b200 when a CUDA device is visible).  There is no CPU sampler in this
