@@ -508,7 +508,9 @@ ksim_status ksim_program_create(ksim_component *const *comps, int32_t n_comps, c
         }
         off += n;
     }
-    for (cudaStream_t *st : {&p->stream, &p->stream_b, &p->s_h2d, &p->s_d2h}) {
+    std::vector<cudaStream_t *> streams = {&p->s_h2d, &p->s_d2h};
+    for (cudaStream_t &st : p->cs) streams.push_back(&st);
+    for (cudaStream_t *st : streams) {
         cudaError_t e = cudaStreamCreateWithFlags(st, cudaStreamNonBlocking);
         if (e != cudaSuccess) {
             ksim_program_destroy(p.release());
@@ -523,7 +525,9 @@ void ksim_program_destroy(ksim_program *p)
 {
     if (!p) return;
     DeviceGuard g(p->device);
-    for (cudaStream_t st : {p->stream, p->stream_b, p->s_h2d, p->s_d2h})
+    std::vector<cudaStream_t> streams = {p->s_h2d, p->s_d2h};
+    for (cudaStream_t st : p->cs) streams.push_back(st);
+    for (cudaStream_t st : streams)
         if (st) cudaStreamSynchronize(st);
     for (auto &part : p->parts) {
         if (part.d_sel) cudaFree(part.d_sel);
@@ -533,8 +537,10 @@ void ksim_program_destroy(ksim_program *p)
     p->ws_out.release();
     p->ws_fp.release();
     p->ws_op.release();
-    for (cudaStream_t st : {p->stream, p->stream_b, p->s_h2d, p->s_d2h})
+    for (cudaStream_t st : streams)
         if (st) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : p->ev_in) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : p->ev_done) cudaEventDestroy(ev);
     delete p;
 }
 
@@ -611,12 +617,36 @@ ksim_status ksim_program_sample_device(ksim_program *p, const uint8_t *d_f_param
 
 namespace {
 
-// Host buffers in, host buffers out, in chunks of shots pipelined over four
-// streams: the f rows of chunk i+1 cross PCIe while chunk i samples, the
-// results of chunk i cross back while chunk i+1 samples, and consecutive
-// chunks alternate between two compute streams so one chunk's last wave of
-// CTAs overlaps the next chunk's first.  Chunk c samples with shot_offset =
-// its first row, so the bits equal a single launch over all B shots.
+// Chunk boundaries of a host call over B shots.  Only the first chunk's
+// input copy and the last chunk's output copy are not hidden behind
+// sampling, so the chunks ramp: u, 2u, then chunks of about 4u, then 2u, u,
+// with u about B / 32 (at least 16 Ki shots, a multiple of 4 Ki).
+std::vector<int64_t> host_chunk_bounds(int64_t B)
+{
+    const int64_t u = std::max<int64_t>((int64_t)1 << 14, (B / 32 + 4095) / 4096 * 4096);
+    std::vector<int64_t> b = {0};
+    if (B <= 6 * u) {  // too few shots to ramp: chunks of u
+        for (int64_t x = u; x < B; x += u) b.push_back(x);
+        b.push_back(B);
+        return b;
+    }
+    b.push_back(u);
+    b.push_back(3 * u);
+    const int64_t body = B - 6 * u, n_body = (body + 4 * u - 1) / (4 * u);
+    const int64_t step = (body / n_body + 4095) / 4096 * 4096;
+    for (int64_t k = 1; k < n_body; ++k) b.push_back(3 * u + k * step);
+    b.push_back(B - 3 * u);
+    b.push_back(B - u);
+    b.push_back(B);
+    return b;
+}
+
+// Host buffers in, host buffers out, in chunks of shots (host_chunk_bounds)
+// pipelined over copy and compute streams: the f rows of chunk i+1 cross
+// PCIe while chunk i samples, the results of chunk i cross back while later
+// chunks sample, and consecutive chunks take the compute streams in turn so
+// their waves of CTAs overlap.  Chunk c samples with shot_offset = its first
+// row, so the bits equal a single launch over all B shots.
 // packed: f rows of ceil(n_f_cols/8) bytes and output rows of
 // ceil(n_outputs/8) bytes, bit c of a row in byte c/8 at bit c%8.
 // noise (nullable): f rows are drawn on the device from this model with
@@ -647,17 +677,23 @@ ksim_status program_sample_host(ksim_program *p, const uint8_t *f, int64_t B, in
     uint8_t *d_in = packed ? (uint8_t *)p->ws_fp.p : d_f;       // where the host rows land
     uint8_t *d_back = packed ? (uint8_t *)p->ws_op.p : d_out;   // what goes back
 
-    // chunks: about a sixth of the shots each, at least 64 Ki shots
-    const int64_t chunk = std::max<int64_t>((int64_t)1 << 16, ((B + 5) / 6 + 4095) / 4096 * 4096);
-    const int n_chunks = (int)((B + chunk - 1) / chunk);
-    std::vector<cudaEvent_t> ev_in(n_chunks, nullptr), ev_done(n_chunks, nullptr);
+    const std::vector<int64_t> bounds = host_chunk_bounds(B);
+    const int n_chunks = (int)bounds.size() - 1;
+    std::vector<cudaEvent_t> &ev_in = p->ev_in, &ev_done = p->ev_done;
     ksim_status st = KSIM_OK;
-    for (int i = 0; i < n_chunks && e == cudaSuccess; ++i) {
-        e = cudaEventCreateWithFlags(&ev_in[i], cudaEventDisableTiming);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_done[i], cudaEventDisableTiming);
+    while ((int)ev_in.size() < n_chunks && e == cudaSuccess) {
+        cudaEvent_t a = nullptr, b = nullptr;
+        e = cudaEventCreateWithFlags(&a, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b, cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            if (a) cudaEventDestroy(a);
+            break;
+        }
+        ev_in.push_back(a);
+        ev_done.push_back(b);
     }
     auto copy_back = [&](int i) -> cudaError_t {
-        const int64_t c0 = (int64_t)i * chunk, n = std::min(chunk, B - c0);
+        const int64_t c0 = bounds[i], n = bounds[i + 1] - c0;
         cudaError_t x = cudaStreamWaitEvent(p->s_d2h, ev_done[i], 0);
         if (x == cudaSuccess)
             x = cudaMemcpyAsync(out + c0 * o_row, d_back + c0 * o_row, (size_t)(n * o_row), cudaMemcpyDeviceToHost,
@@ -665,8 +701,8 @@ ksim_status program_sample_host(ksim_program *p, const uint8_t *f, int64_t B, in
         return x;
     };
     for (int i = 0; i < n_chunks && e == cudaSuccess && st == KSIM_OK; ++i) {
-        const int64_t c0 = (int64_t)i * chunk, n = std::min(chunk, B - c0);
-        cudaStream_t cs = (i & 1) ? p->stream_b : p->stream;
+        const int64_t c0 = bounds[i], n = bounds[i + 1] - c0;
+        cudaStream_t cs = p->cs[i % KSIM_HOST_STREAMS];
         if (noise) {
             e = launch_noise(noise, n, c0, noise_seed, d_f + c0 * n_f_cols, n_f_cols, cs);
         } else {
@@ -687,13 +723,14 @@ ksim_status program_sample_host(ksim_program *p, const uint8_t *f, int64_t B, in
         if (e == cudaSuccess && i > 0) e = copy_back(i - 1);  // after chunk i is queued
     }
     if (e == cudaSuccess && st == KSIM_OK) e = copy_back(n_chunks - 1);
-    for (cudaStream_t x : {p->s_h2d, p->stream, p->stream_b, p->s_d2h}) {
-        const cudaError_t y = cudaStreamSynchronize(x);
-        if (e == cudaSuccess) e = y;
-    }
-    for (int i = 0; i < n_chunks; ++i) {
-        if (ev_in[i]) cudaEventDestroy(ev_in[i]);
-        if (ev_done[i]) cudaEventDestroy(ev_done[i]);
+    if (e == cudaSuccess && st == KSIM_OK) {
+        // every chunk's output copy waited for its sampling, which waited for
+        // its input copy: the output stream's end is the call's end
+        e = cudaStreamSynchronize(p->s_d2h);
+    } else {
+        std::vector<cudaStream_t> streams = {p->s_h2d, p->s_d2h};
+        for (cudaStream_t x : p->cs) streams.push_back(x);
+        for (cudaStream_t x : streams) cudaStreamSynchronize(x);
     }
     if (st != KSIM_OK) return st;
     if (e != cudaSuccess) return cuda_fail(e, "program sample");

@@ -61,14 +61,19 @@ struct ProgramPart {
     int32_t *d_cols = nullptr;  // destination output column of each component output
 };
 
+#ifndef KSIM_HOST_STREAMS
+#define KSIM_HOST_STREAMS 4
+#endif
+
 struct ksim_program {
     int device = 0;
     int n_outputs = 0;
     int min_f_cols = 0;
     std::vector<ProgramPart> parts;
-    // host-buffer calls: two compute streams (chunk tails overlap) and one
-    // stream per copy direction
-    cudaStream_t stream = nullptr, stream_b = nullptr, s_h2d = nullptr, s_d2h = nullptr;
+    // host-buffer calls: KSIM_HOST_STREAMS compute streams taken in turn
+    // (consecutive chunks overlap) and one stream per copy direction
+    cudaStream_t cs[KSIM_HOST_STREAMS] = {}, s_h2d = nullptr, s_d2h = nullptr;
+    std::vector<cudaEvent_t> ev_in, ev_done;  // per chunk, kept across calls
     ksim::DevBuf ws_f, ws_out, ws_fp, ws_op;  // unpacked rows; bit-packed rows
     std::mutex mu;
 };

@@ -1,7 +1,8 @@
 """Host-buffer sampling: chunked, copy-overlapped calls and bit-packed I/O.
 
-ksim_program_sample splits large calls into chunks of shots whose copies
-overlap the neighbouring chunks' sampling; each chunk samples with its first
+ksim_program_sample splits large calls into chunks of shots (small first and
+last chunks, larger ones between) whose copies overlap other chunks'
+sampling; each chunk samples with its first
 row as shot offset, so the bits must equal one device launch over all shots
 (and the oracle).  ksim_program_sample_packed takes and returns rows packed
 8 columns per byte; its bits must equal the byte-per-bit call's.
@@ -39,7 +40,20 @@ def _device_once(sampler, f, seed, mode):
     return d_out.cpu().numpy()
 
 
-@pytest.mark.parametrize("B", [1, 1000, 65536, 65537, 131073, 700_001])
+def _chunk_bounds(B):
+    """The host call's chunk schedule (api.cu host_chunk_bounds): u, 2u,
+    chunks of about 4u, 2u, u with u ~ B / 32 (>= 16 Ki, a multiple of 4 Ki),
+    or chunks of u when B <= 6u."""
+    u = max(1 << 14, (B // 32 + 4095) // 4096 * 4096)
+    if B <= 6 * u:
+        return list(range(0, B, u)) + [B]
+    body = B - 6 * u
+    n_body = -(-body // (4 * u))
+    step = (body // n_body + 4095) // 4096 * 4096
+    return [0, u] + [3 * u + k * step for k in range(n_body)] + [B - 3 * u, B - u, B]
+
+
+@pytest.mark.parametrize("B", [1, 1000, 65536, 65537, 98305, 131073, 700_001])
 def test_chunked_host_call_equals_one_launch(cuda_device, oracle_port, small_prog, B):
     from ksim_b200.sampler import B200ProgramSampler
     rng, prog, n_f = small_prog
@@ -48,12 +62,14 @@ def test_chunked_host_call_equals_one_launch(cuda_device, oracle_port, small_pro
     for mode in (0, 1):
         got = s.sample(f, 31 + B, rng_mode=mode)
         assert np.array_equal(got, _device_once(s, f, 31 + B, mode)), mode
-    # spot-check against the oracle at the chunk seams
-    for lo in sorted({0, max(0, B - 300), max(0, min(B, 65536) - 150), max(0, min(B, 131072) - 150)}):
-        lo = max(lo, 0)
+    # spot-check against the oracle across the chunk seams
+    bounds = _chunk_bounds(B)
+    assert all(x < y for x, y in zip(bounds, bounds[1:])) and bounds[-1] == B
+    got = s.sample(f, 31 + B, rng_mode=1)
+    for lo in sorted({max(0, x - 150) for x in bounds}):
         hi = min(B, lo + 300)
         want = oracle_port.program_sample(prog, f[lo:hi], 31 + B, rng_mode=1, shot_offset=lo)
-        assert np.array_equal(s.sample(f, 31 + B, rng_mode=1)[lo:hi], want), lo
+        assert np.array_equal(got[lo:hi], want), lo
 
 
 @pytest.mark.parametrize("B", [5, 4096, 300_000])
