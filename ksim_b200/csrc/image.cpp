@@ -8,7 +8,10 @@
 //   i32 power2, i32 floatfactor[4], u32 n0 | n2<<16, u32 n1 | n3<<16 (the
 //   NodePhases columns per rotation class), i32 H (the block's halvings),
 //   u32 record bytes, u64 C[4] (the block's all-plus product / 2^H, mod
-//   2^64), u32 nb (parity blocks), u32 0, u64 0,
+//   2^64), u32 nb (parity blocks), and for a fast term its layout: u16
+//   offsets / 16 of the PhasePairs tables, step tables, lambda table and
+//   parity blocks, u16 first PhasePairs row, u16 nu0 | constants' offset / 16
+//   << 2 (zeros for an exact term),
 // then [f64 approx re, im], then the body.  A fast term's body is its parity
 // rows (layout: zring.cuh).  An exact (TF_SLOW) term's body is the columns
 // in the reference's order, each the parameter masks as W 64-bit words (bit j
@@ -610,6 +613,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             if (g.pf_has_approx) flags |= TF_APX;
             std::vector<uint8_t> body;  // everything after the header (and approximation)
             uint32_t nb = 0, sum_iter = 0;
+            size_t blocks_at = 0;       // where the parity blocks start in body
             if (unsafe) {
                 // the reference's column order and layout
                 for (int c = 0; c < cnp; ++c) {
@@ -658,6 +662,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                     }
                 }
                 while (body.size() & 15u) body.push_back(0);
+                blocks_at = body.size();
                 nb = (uint32_t)((rows.size() + 31) / 32);
                 const uint16_t zero_off = (uint16_t)(8 * 64 * W);
                 for (uint32_t b = 0; b < nb; ++b) {
@@ -705,9 +710,29 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             put32(out, unsafe ? 0u : (uint32_t)np_halvings);
             put32(out, (uint32_t)rec_bytes);
             for (int k = 0; k < 4; ++k) put64(out, unsafe ? 0ull : (uint64_t)C[k]);
+            // a fast term's layout as its reader takes it: part offsets in
+            // 16-byte units, the first PhasePairs row, the NodePhases
+            // valuation mod 4 and the constants' offset
+            uint32_t lay[3] = {0u, 0u, 0u};
+            if (!unsafe) {
+                TermHdr lh = {};
+                lh.n_np = (uint32_t)n_np; lh.n_hp = (uint32_t)n_hp; lh.n_pp = (uint32_t)n_pp; lh.n_ph = (uint32_t)n_ph;
+                lh.flags = flags;
+                lh.n_cls[0] = (uint32_t)n_cls[0]; lh.n_cls[1] = (uint32_t)n_cls[2];  // run order j = 0, 2, 1, 3
+                lh.n_cls[2] = (uint32_t)n_cls[1]; lh.n_cls[3] = (uint32_t)n_cls[3];
+                const int meta = layout_meta_off(lh), tab = layout_pair_tab_off(lh), step = layout_pair_step_off(lh);
+                const int npl = layout_npl_off(lh), blk = layout_blocks_off(lh), row0 = layout_ph_row0(lh);
+                if (blk != meta + (int)blocks_at || ((meta | tab | step | npl | blk) & 15) || blk >= (1 << 20) ||
+                    row0 > 0xFFFF) {
+                    err = gname + ": internal error: term layout";
+                    return KSIM_ERR_UNSUPPORTED;
+                }
+                lay[0] = (uint32_t)(tab >> 4) | ((uint32_t)(step >> 4) << 16);
+                lay[1] = (uint32_t)(npl >> 4) | ((uint32_t)(blk >> 4) << 16);
+                lay[2] = (uint32_t)row0 | (layout_nu0(lh) << 16) | ((uint32_t)(meta >> 4) << 18);
+            }
             put32(out, nb);
-            put32(out, 0u);
-            put64(out, 0u);
+            for (uint32_t x : lay) put32(out, x);
             if (g.pf_has_approx) {
                 double ar = g.pf_approx_f32[2 * (size_t)t], ai = g.pf_approx_f32[2 * (size_t)t + 1];
                 uint64_t u;

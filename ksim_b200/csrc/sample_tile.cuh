@@ -239,6 +239,13 @@ __device__ __forceinline__ void ballot_words(uint64_t *sw, const uint64_t (&vk)[
     __syncwarp();
 }
 
+// Ballot words of positions [k0, k1) that hold the same bit for every shot
+// (x = all ones or zero); the caller syncs the warp.
+__device__ __forceinline__ void uniform_words(uint64_t *sw, int k0, int k1, uint64_t x, int lane)
+{
+    for (int k = k0 + lane; k < k1; k += 32) sw[k] = x;
+}
+
 // The exact path out of line: rare, and inlined it would take registers from
 // the fast path of every term.
 template <int W>
@@ -474,13 +481,24 @@ __device__ __forceinline__ bool sample_tile(const SampleJob &j, const int64_t s0
                 sim[r] = 0.0;
             }
             if (k + 1 < j.n_graphs) {
-                // bits [F + nm_k, max(P_k, P_k+1)) change: the output just
-                // sampled replaces its trying bit, the trying range follows P
+                // graph k + 1's vector: [0, lo) from v, trying bits [lo, Pn)
+                // = 1, zeros above (lo = F + k).  Against graph k's only the
+                // output just sampled (position lo - 1, k >= 1) differs
+                // between shots: it gets a ballot.  The trying bits that
+                // enter ([max(lo, P_k), Pn); all of [lo, Pn) after graph 0,
+                // which has none) and the positions that leave the vector
+                // ([max(lo, Pn), P_k)) are the same for every shot: their
+                // words are written whole.  The top bit (the constant 1)
+                // stays.
                 const int Pn = graph_params<CG>(j.gdir + k + 1);
 #pragma unroll
                 for (int r = 0; r < S; ++r) graph_vector<W>(vk[r], v[r], F, k + 1, Pn);
-                const int lo = F + (k > 0 ? k - 1 : 0), hi = Pk > Pn ? Pk : Pn;
-                ballot_words<W, S>(sw, vk, lo, hi < 64 * W - 1 ? hi : 64 * W - 1, lane);
+                const int top = 64 * W - 1, lo = F + k;
+                const int on0 = k > 0 ? max(lo, Pk) : lo;
+                uniform_words(sw, on0, min(Pn, top), ~0ull, lane);
+                uniform_words(sw, max(lo, Pn), min(Pk, top), 0ull, lane);
+                if (k > 0 && lo - 1 < top) ballot_words<W, S>(sw, vk, lo - 1, lo, lane);  // ends with a warp sync
+                else __syncwarp();
                 Pk = Pn;
             }
         }

@@ -256,6 +256,11 @@ struct TermHdr {
     int32_t np_pw;      // halvings of the NodePhases block (a term that survives it)
     uint32_t rec_bytes; // the whole term record
     uint32_t nb;          // 32-row parity blocks (fast terms)
+    // fast terms: byte offsets of the record's parts (written by the packer
+    // from the layout_* functions below, so a shot reads them instead of
+    // deriving them from the counts), the first PhasePairs row and the
+    // valuation of the NodePhases result mod 4
+    uint32_t off_meta, off_tab, off_step, off_npl, off_blk, ph_row0, nu0;
 };
 // The NodePhases constant C (4 x 64-bit words, mod 2^64) follows the header
 // fields at this offset.
@@ -273,7 +278,7 @@ KS_HD void set_one_bit(uint64_t (&v)[W])
 
 KS_HD TermHdr load_hdr(const uint8_t *p)
 {
-    uint32_t u[12], nb;
+    uint32_t u[12], nb, lay[3];
 #if defined(__CUDA_ARCH__)
     const uint4 *q = (const uint4 *)p;  // records are 16-byte aligned
 #pragma unroll
@@ -281,11 +286,13 @@ KS_HD TermHdr load_hdr(const uint8_t *p)
         const uint4 x = q[i];
         u[4 * i] = x.x; u[4 * i + 1] = x.y; u[4 * i + 2] = x.z; u[4 * i + 3] = x.w;
     }
-    nb = q[5].x;
+    const uint4 t = q[5];
+    nb = t.x; lay[0] = t.y; lay[1] = t.z; lay[2] = t.w;
 #else
     const uint32_t *q = (const uint32_t *)p;
     for (int i = 0; i < 12; ++i) u[i] = q[i];
     nb = q[20];
+    lay[0] = q[21]; lay[1] = q[22]; lay[2] = q[23];
 #endif
     TermHdr h;
     h.n_np = u[0] & 0xFFFFu; h.n_hp = u[0] >> 16;
@@ -299,6 +306,13 @@ KS_HD TermHdr load_hdr(const uint8_t *p)
     h.np_pw = (int32_t)u[10];
     h.rec_bytes = u[11];
     h.nb = nb;
+    h.off_tab = (lay[0] & 0xFFFFu) << 4;
+    h.off_step = (lay[0] >> 16) << 4;
+    h.off_npl = (lay[1] & 0xFFFFu) << 4;
+    h.off_blk = (lay[1] >> 16) << 4;
+    h.ph_row0 = lay[2] & 0xFFFFu;
+    h.nu0 = (lay[2] >> 16) & 3u;
+    h.off_meta = (lay[2] >> 18) << 4;
     return h;
 }
 
@@ -408,7 +422,7 @@ struct TermOut {
 // times w^(k + phase index) for k = 0..7 (8 x 4 i32, so the final rotation
 // and the floatfactor are one table read and one product), u16 dead_pw per
 // class-0 row, padded to 16 bytes; the PhasePairs pair tables and valuation
-// words (see term_pair_tab_off), each part padded to 16 bytes; then nb
+// words (see layout_pair_tab_off), each part padded to 16 bytes; then nb
 // blocks of 32 rows, each a 32-byte head
 //   u32 n_pairs, u32 masks P1, P2, P4, E3, E1, PP, K0 (bit i = row 32b + i)
 // and n_pairs x 32 u32 words of two u16 byte offsets (8 x bit index; word
@@ -423,7 +437,6 @@ struct TermOut {
 //     (= m3 - m1 with E3 / E1 the class-3 / class-1 rows)
 //   kill: the first row of w & K0 (class 0) with its dead_pw.
 constexpr int BLOCK_HEAD_BYTES = 32;
-KS_HD int term_meta_off(const TermHdr &h) { return TERM_HDR_BYTES + ((h.flags & TF_APX) ? TERM_APX_BYTES : 0); }
 constexpr int TERM_FFK_BYTES = 128;
 // PhasePairs columns 2p and 2p + 1 run as one pair (an odd last column
 // pairs with the factor 1, its sign bits being rows past the end, which are
@@ -433,24 +446,47 @@ constexpr int TERM_FFK_BYTES = 128;
 // and the packer sends terms that can leave that range to the exact path) of
 // z before the pair, holds the pair's halvings (bits 0-1), the valuation
 // after it (bits 2-5) and whether z stays nonzero (bit 6).
-KS_HD uint32_t term_ph_pairs(const TermHdr &h) { return (h.n_ph + 1) >> 1; }
-KS_HD int term_pair_tab_off(const TermHdr &h)
+// NodePhases products C lambda^e, e = -n1 .. n3, follow for terms with
+// class-1 or class-3 columns (n_cls[2], n_cls[3] in run order): 4 x u32 per
+// entry on the 32-bit NodePhases paths, 4 x u64 otherwise; entry i is
+// e = i - n1.
+//
+// The layout from the counts (the packer places the parts with these and
+// stores the offsets in the header) ...
+KS_HD int layout_meta_off(const TermHdr &h) { return TERM_HDR_BYTES + ((h.flags & TF_APX) ? TERM_APX_BYTES : 0); }
+KS_HD uint32_t layout_ph_pairs(const TermHdr &h) { return (h.n_ph + 1) >> 1; }
+KS_HD int layout_pair_tab_off(const TermHdr &h)
 {
-    return term_meta_off(h) + TERM_FFK_BYTES + ((2 * (int)h.n_cls[0] + 15) & ~15);
+    return layout_meta_off(h) + TERM_FFK_BYTES + ((2 * (int)h.n_cls[0] + 15) & ~15);
 }
-KS_HD int term_pair_step_off(const TermHdr &h) { return term_pair_tab_off(h) + 64 * (int)term_ph_pairs(h); }
-// NodePhases products C lambda^e, e = -n1 .. n3, for terms with class-1 or
-// class-3 columns (n_cls[2], n_cls[3] in run order): 4 x u32 per entry on the
-// 32-bit NodePhases paths, 4 x u64 otherwise; entry i is e = i - n1.
-KS_HD bool term_np_odd(const TermHdr &h) { return (h.n_cls[2] | h.n_cls[3]) != 0; }
-KS_HD int term_npl_off(const TermHdr &h) { return term_pair_step_off(h) + 256 * (int)term_ph_pairs(h); }
-KS_HD int term_npl_bytes(const TermHdr &h)
+KS_HD int layout_pair_step_off(const TermHdr &h) { return layout_pair_tab_off(h) + 64 * (int)layout_ph_pairs(h); }
+KS_HD bool layout_np_odd(const TermHdr &h) { return (h.n_cls[2] | h.n_cls[3]) != 0; }
+KS_HD int layout_npl_off(const TermHdr &h) { return layout_pair_step_off(h) + 256 * (int)layout_ph_pairs(h); }
+KS_HD int layout_npl_bytes(const TermHdr &h)
 {
-    if (!term_np_odd(h)) return 0;
+    if (!layout_np_odd(h)) return 0;
     const int entry = (h.flags & (TF_NARROW | TF_HYBRID)) ? 16 : 32;
     return ((int)(h.n_cls[2] + h.n_cls[3] + 1) * entry + 15) & ~15;
 }
-KS_HD int term_blocks_off(const TermHdr &h) { return term_npl_off(h) + term_npl_bytes(h); }
+KS_HD int layout_blocks_off(const TermHdr &h) { return layout_npl_off(h) + layout_npl_bytes(h); }
+// Position of the first PhasePairs row.
+KS_HD int layout_ph_row0(const TermHdr &h)
+{
+    const int pp0 = ((int)(h.n_np + h.n_hp) + 1) & ~1;
+    return (pp0 + 2 * (int)h.n_pp + 3) & ~3;  // pairs of PhasePairs columns: 4-bit aligned
+}
+// Valuation mod 4 of the NodePhases result: (2 n2 + n1 + n3) mod 4.
+KS_HD uint32_t layout_nu0(const TermHdr &h) { return (2u * h.n_cls[1] + h.n_cls[2] + h.n_cls[3]) & 3u; }
+
+// ... and as a record's reader takes it from the header.
+KS_HD int term_meta_off(const TermHdr &h) { return (int)h.off_meta; }
+KS_HD int term_pair_tab_off(const TermHdr &h) { return (int)h.off_tab; }
+KS_HD int term_pair_step_off(const TermHdr &h) { return (int)h.off_step; }
+KS_HD uint32_t term_ph_pairs(const TermHdr &h) { return (h.off_npl - h.off_step) >> 8; }  // 256 step bytes a pair
+KS_HD int term_npl_off(const TermHdr &h) { return (int)h.off_npl; }
+KS_HD bool term_np_odd(const TermHdr &h) { return h.off_blk != h.off_npl; }
+KS_HD int term_blocks_off(const TermHdr &h) { return (int)h.off_blk; }
+KS_HD int term_ph_row0(const TermHdr &h) { return (int)h.ph_row0; }
 
 // Entry i of a term's lambda table in the word type of its NodePhases block.
 KS_HD Zr<uint32_t> load_npl(const uint8_t *tab, uint32_t i, uint32_t)
@@ -483,12 +519,6 @@ KS_HD void load_i32x4(const uint8_t *p, int32_t (&r)[4])
     const int32_t *q = (const int32_t *)p;
     r[0] = q[0]; r[1] = q[1]; r[2] = q[2]; r[3] = q[3];
 #endif
-}
-// Position of the first PhasePairs row.
-KS_HD int term_ph_row0(const TermHdr &h)
-{
-    const int pp0 = ((int)(h.n_np + h.n_hp) + 1) & ~1;
-    return (pp0 + 2 * (int)h.n_pp + 3) & ~3;  // pairs of PhasePairs columns: 4-bit aligned
 }
 
 KS_HD uint32_t popc32(uint32_t x)
@@ -654,7 +684,7 @@ KS_HD const uint8_t *eval_term_rows(const uint8_t *p, const TermHdr &h, const Ro
         const uint8_t *pstep = p + term_pair_step_off(h);
         uint32_t nu[S];
 #pragma unroll
-        for (int s = 0; s < S; ++s) nu[s] = (2u * h.n_cls[1] + h.n_cls[2] + h.n_cls[3]) & 3u;
+        for (int s = 0; s < S; ++s) nu[s] = h.nu0;
         for (uint32_t q = 0; q < n_pair; ++q) {
             const int pos = ph0 + 4 * (int)q;
 #pragma unroll
