@@ -581,28 +581,81 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
             std::vector<const std::vector<uint64_t> *> rows;
             std::vector<uint32_t> role;  // mask bits of each row
             const std::vector<uint64_t> zero_row((size_t)W, 0);
+            int ph_row0 = 0;
             if (!unsafe) {
+                // class-0 NodePhases rows first, in column order: the kill
+                // takes the first that fires, and dead_pw is indexed by
+                // position.  Then the other NodePhases and the HalfPi rows
+                // (single rows) and the PiProducts (psi, phi) pairs (at even
+                // positions, so a pair never straddles a block), heaviest
+                // first: a block's row loop runs as many index pairs as its
+                // row with the most set bits, so grouping the long rows
+                // shortens the other blocks' loops.  The PhasePairs pairs
+                // follow from a multiple of 4, in column order.
+                auto bits = [&](const std::vector<uint64_t> &m) {
+                    int n = 0;
+                    for (uint64_t x : m) n += __builtin_popcountll(x);
+                    return n;
+                };
+                struct Unit { int weight, first; uint32_t role0; bool pair; const std::vector<uint64_t> *m0; };
+                std::vector<Unit> singles, doubles;
                 for (int r = 0; r < cnp; ++r) {
                     const uint32_t j = npc[order[r]].phase & 3u;
-                    rows.push_back(&npc[order[r]].m);
-                    role.push_back(j == 0 ? R_K0 : (R_P2 | R_P4 | (j == 3 ? R_E3 : j == 1 ? R_E1 : 0u)));
+                    if (j == 0) {
+                        rows.push_back(&npc[order[r]].m);
+                        role.push_back(R_K0);
+                    } else {
+                        singles.push_back({bits(npc[order[r]].m), r, R_P2 | R_P4 | (j == 3 ? R_E3 : j == 1 ? R_E1 : 0u),
+                                           false, &npc[order[r]].m});
+                    }
                 }
-                for (const Row &h : hp_rows) {
-                    rows.push_back(&h.m);
-                    role.push_back(((h.c & 1u) ? R_P1 : 0u) | ((h.c & 2u) ? R_P2 : 0u) | ((h.c & 4u) ? R_P4 : 0u));
+                for (size_t i = 0; i < hp_rows.size(); ++i) {
+                    const Row &h = hp_rows[i];
+                    singles.push_back({bits(h.m), cnp + (int)i,
+                                       ((h.c & 1u) ? R_P1 : 0u) | ((h.c & 2u) ? R_P2 : 0u) | ((h.c & 4u) ? R_P4 : 0u),
+                                       false, &h.m});
                 }
-                if (rows.size() & 1u) {
-                    rows.push_back(&zero_row);
-                    role.push_back(0u);
-                }
-                for (size_t i = 0; i < pair_rows.size(); ++i) {
+                for (size_t i = 0; i + 1 < pair_rows.size(); i += 2)
+                    doubles.push_back({std::max(bits(pair_rows[i].m), bits(pair_rows[i + 1].m)), (int)i, R_PP, true,
+                                       &pair_rows[i].m});
+                auto heavier = [](const Unit &x, const Unit &y) {
+                    return x.weight != y.weight ? x.weight > y.weight : x.first < y.first;
+                };
+                std::sort(singles.begin(), singles.end(), heavier);
+                std::sort(doubles.begin(), doubles.end(), heavier);
+                size_t si = 0, di = 0;
+                auto put_single = [&]() {
+                    rows.push_back(singles[si].m0);
+                    role.push_back(singles[si].role0);
+                    ++si;
+                };
+                while (si < singles.size() || di < doubles.size()) {
+                    const bool take_pair = di < doubles.size() &&
+                                           (si == singles.size() || heavier(doubles[di], singles[si]));
+                    if (!take_pair) {
+                        put_single();
+                        continue;
+                    }
+                    if (rows.size() & 1u) {  // a pair starts at an even position
+                        if (si < singles.size()) {
+                            put_single();
+                        } else {
+                            rows.push_back(&zero_row);
+                            role.push_back(0u);
+                        }
+                    }
+                    const size_t i = (size_t)doubles[di].first;
                     rows.push_back(&pair_rows[i].m);
-                    role.push_back((i & 1u) ? 0u : R_PP);
+                    role.push_back(R_PP);
+                    rows.push_back(&pair_rows[i + 1].m);
+                    role.push_back(0u);
+                    ++di;
                 }
                 while (rows.size() & 3u) {  // PhasePairs pairs: 4-bit aligned
                     rows.push_back(&zero_row);
                     role.push_back(0u);
                 }
+                ph_row0 = (int)rows.size();
                 for (const Row &q : ph_rows) {
                     rows.push_back(&q.m);
                     role.push_back(0u);
@@ -610,6 +663,20 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 if (rows.size() > (size_t)32 * NB_MAX) unsafe = true;
             }
             if (unsafe) flags = TF_SLOW;
+            if (!unsafe) {
+                // the scales 2^(pw + power2) a shot can reach: pw starts at
+                // H or at a kill's dead_pw and gains at most two halvings per
+                // PhasePairs pair and one renormalisation
+                int64_t lo = np_halvings, hi = np_halvings;
+                for (int c = 0; c < cnp; ++c)
+                    if ((npc[c].phase & 3u) == 0) {
+                        lo = std::min<int64_t>(lo, dead_pw[c]);
+                        hi = std::max<int64_t>(hi, dead_pw[c]);
+                    }
+                hi += 2 * (int64_t)((n_ph + 1) / 2) + 1;
+                const int64_t p2 = g.pf_power2[t];
+                if (p2 + lo >= -1022 && p2 + hi <= 1023) flags |= TF_EXP;
+            }
             if (g.pf_has_approx) flags |= TF_APX;
             std::vector<uint8_t> body;  // everything after the header (and approximation)
             uint32_t nb = 0, sum_iter = 0;
@@ -721,7 +788,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 lh.n_cls[0] = (uint32_t)n_cls[0]; lh.n_cls[1] = (uint32_t)n_cls[2];  // run order j = 0, 2, 1, 3
                 lh.n_cls[2] = (uint32_t)n_cls[1]; lh.n_cls[3] = (uint32_t)n_cls[3];
                 const int meta = layout_meta_off(lh), tab = layout_pair_tab_off(lh), step = layout_pair_step_off(lh);
-                const int npl = layout_npl_off(lh), blk = layout_blocks_off(lh), row0 = layout_ph_row0(lh);
+                const int npl = layout_npl_off(lh), blk = layout_blocks_off(lh), row0 = ph_row0;
                 if (blk != meta + (int)blocks_at || ((meta | tab | step | npl | blk) & 15) || blk >= (1 << 20) ||
                     row0 > 0xFFFF) {
                     err = gname + ": internal error: term layout";

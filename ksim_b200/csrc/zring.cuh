@@ -57,7 +57,11 @@ namespace ksim {
 // and at the end) is proven below 2^31, so it runs on 32-bit coefficients.
 // TF_HYBRID: the NodePhases block is proven below 2^31 and runs on 32-bit
 // words, the rest on 64-bit words.
-enum : uint32_t { TF_SLOW = 1u, TF_APX = 2u, TF_NARROW = 4u, TF_HYBRID = 8u };
+// TF_EXP: every scale 2^(pw + power2) the fast term can reach (pw from the
+// NodePhases halvings or a kill's dead_pw, plus at most two halvings per
+// PhasePairs pair and one renormalisation) is a normal double, so the scale
+// is built from its exponent bits without pow2i's range tests.
+enum : uint32_t { TF_SLOW = 1u, TF_APX = 2u, TF_NARROW = 4u, TF_HYBRID = 8u, TF_EXP = 16u };
 constexpr int TERM_HDR_BYTES = 96;
 constexpr int TERM_APX_BYTES = 16;
 // NodePhases / HalfPi column: W mask words + 1 constant word, padded to 16 B
@@ -149,6 +153,16 @@ KS_HD double pow2i(int64_t n)
     if (n >= -1022) return bits_to_double((uint64_t)(n + 1023) << 52);
     if (n >= -1074) return bits_to_double(1ull << (n + 1074));
     return 0.0;
+}
+
+// 2^n for n in [-1022, 1023] (a normal double: exponent field n + 1023).
+KS_HD double pow2_normal(int32_t n)
+{
+#if defined(__CUDA_ARCH__)
+    return __hiloint2double((n + 1023) << 20, 0);
+#else
+    return bits_to_double((uint64_t)(n + 1023) << 52);
+#endif
 }
 
 // z * w^k for a per-shot k in 0..7 (selects, no branches).
@@ -415,9 +429,11 @@ struct TermOut {
 // ---- fast terms: parity rows -------------------------------------------------
 // A fast term's columns are parity rows over the parameter vector, each
 // stored as the list of its set bits.  Row order (term-relative position):
-//   NodePhases class 0, 2, 1, 3 | HalfPi | (a zero row if needed to make the
-//   next position even) | PiProducts (psi, phi) pairs | (zero rows to a
-//   multiple of 4) | PhasePairs (alpha, beta) pairs
+//   NodePhases class 0 in column order | the other NodePhases rows, the
+//   HalfPi rows and the PiProducts (psi, phi) pairs (each pair at an even
+//   position, a zero row where needed), the rows with the most set bits
+//   first | (zero rows to a multiple of 4: the header's ph_row0) |
+//   PhasePairs (alpha, beta) pairs in column order
 // After the header (and approximation) the term's constants: the floatfactor
 // times w^(k + phase index) for k = 0..7 (8 x 4 i32, so the final rotation
 // and the floatfactor are one table read and one product), u16 dead_pw per
@@ -469,12 +485,6 @@ KS_HD int layout_npl_bytes(const TermHdr &h)
     return ((int)(h.n_cls[2] + h.n_cls[3] + 1) * entry + 15) & ~15;
 }
 KS_HD int layout_blocks_off(const TermHdr &h) { return layout_npl_off(h) + layout_npl_bytes(h); }
-// Position of the first PhasePairs row.
-KS_HD int layout_ph_row0(const TermHdr &h)
-{
-    const int pp0 = ((int)(h.n_np + h.n_hp) + 1) & ~1;
-    return (pp0 + 2 * (int)h.n_pp + 3) & ~3;  // pairs of PhasePairs columns: 4-bit aligned
-}
 // Valuation mod 4 of the NodePhases result: (2 n2 + n1 + n3) mod 4.
 KS_HD uint32_t layout_nu0(const TermHdr &h) { return (2u * h.n_cls[1] + h.n_cls[2] + h.n_cls[3]) & 3u; }
 
@@ -518,6 +528,22 @@ KS_HD void load_i32x4(const uint8_t *p, int32_t (&r)[4])
 #else
     const int32_t *q = (const int32_t *)p;
     r[0] = q[0]; r[1] = q[1]; r[2] = q[2]; r[3] = q[3];
+#endif
+}
+
+// Byte B of x as a signed 32-bit value.  On the device one byte permute:
+// a selector nibble with its top bit set copies the sign bit of the byte it
+// names into every bit of the result byte (PTX prmt, default mode).
+template <int B>
+KS_HD int32_t sext_byte(uint32_t x)
+{
+#if defined(__CUDA_ARCH__)
+    constexpr uint32_t sel = (uint32_t)B | ((uint32_t)(8 | B) * 0x1110u);
+    uint32_t r;
+    asm("prmt.b32 %0, %1, 0, %2;" : "=r"(r) : "r"(x), "n"(sel));
+    return (int32_t)r;
+#else
+    return (int32_t)(x << (24 - 8 * B)) >> 24;
 #endif
 }
 
@@ -696,8 +722,8 @@ KS_HD const uint8_t *eval_term_rows(const uint8_t *p, const TermHdr &h, const Ro
                 alive[s] &= e >> 6;
                 nu[s] = (e >> 2) & 15u;
                 const uint32_t fw = *(const uint32_t *)(ptab + 64 * q + 4 * c);  // 4 x i8
-                const Zr<T> F = {(T)(int64_t)((int32_t)(fw << 24) >> 24), (T)(int64_t)((int32_t)(fw << 16) >> 24),
-                                 (T)(int64_t)((int32_t)(fw << 8) >> 24), (T)(int64_t)((int32_t)fw >> 24)};
+                const Zr<T> F = {(T)(int64_t)sext_byte<0>(fw), (T)(int64_t)sext_byte<1>(fw),
+                                 (T)(int64_t)sext_byte<2>(fw), (T)(int64_t)sext_byte<3>(fw)};
                 z[s] = zmul(z[s], F);
                 shr_all(z[s], hh);
                 pw[s] += (int32_t)hh;
@@ -806,7 +832,7 @@ KS_HD void term_complex(const TermOut &o, const uint8_t *hdr_ptr, uint32_t flags
     const double C = (double)(int64_t)o.z.c, D = (double)(int64_t)o.z.d;
     re = dadd(A, dmul(dadd(Bv, D), SQ));
     im = dadd(C, dmul(dsub(Bv, D), SQ));
-    const double s = pow2i(o.pw + (int64_t)o.power2);
+    const double s = (flags & TF_EXP) ? pow2_normal((int32_t)o.pw + o.power2) : pow2i(o.pw + (int64_t)o.power2);
     re = dmul(re, s);
     im = dmul(im, s);
     if (flags & TF_APX) {
