@@ -493,15 +493,16 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                 fs[nu] = L_np;
                 for (size_t q = 0; q < n_pair; ++q) {
                     // step table: entry 16 c + nu (c = the pair's four sign
-                    // bits, nu = the valuation of z before the pair, 0..15)
-                    // holds the pair's halvings h1 + h2 (bits 0-1), nu after
-                    // it (bits 2-5) and whether z stays nonzero (bit 6): the
-                    // reference halves after a factor iff nu(z) >= 4, and a
-                    // zero factor stops the halvings from where it acts.  A
-                    // factor can have nu up to 6, so nu may grow; terms whose
-                    // reachable nu leaves 0..15 take the exact path.
+                    // bits, nu = the valuation of z before the pair, 0..14,
+                    // or NU_DEAD: z is zero) holds the pair's halvings
+                    // h1 + h2 (bits 0-1) and the state after it (bits 2-5):
+                    // the reference halves after a factor iff nu(z) >= 4,
+                    // and a zero factor stops the halvings from where it
+                    // acts (NU_DEAD absorbs, with no halvings).  A factor can
+                    // have nu up to 6, so nu may grow; terms whose reachable
+                    // nu leaves 0..14 take the exact path.
                     for (const auto &sv : fs)
-                        if (sv.first > 15) pair_ok = false;
+                        if (sv.first >= NU_DEAD) pair_ok = false;
                     const uint32_t second = 2 * q + 1 < (size_t)n_ph ? 1u : 0u;
                     for (uint32_t c = 0; c < 16; ++c) {
                         int64_t f1[4], f2[4];
@@ -509,16 +510,17 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                         ph_factor2(2 * q + 1, c >> 2, f2);
                         const uint32_t v1 = std::min<uint32_t>(zw_valuation(f1), 15u);
                         const uint32_t v2 = std::min<uint32_t>(zw_valuation(f2), 15u);
-                        for (uint32_t nu0 = 0; nu0 < 16; ++nu0) {
+                        pair_step[256 * q + 16 * c + NU_DEAD] = (uint8_t)(NU_DEAD << 2);
+                        for (uint32_t nu0 = 0; nu0 < NU_DEAD; ++nu0) {
                             uint32_t alive = v1 != 15 ? 1u : 0u;
                             uint32_t tt = nu0 + v1;
                             const uint32_t h1 = (tt >= 4 ? 1u : 0u) & alive;
                             alive &= v2 != 15 ? 1u : 0u;
                             tt = tt - 4 * h1 + v2;
                             const uint32_t h2 = (tt >= 4 ? 1u : 0u) & alive & second;
-                            const uint32_t nu1 = alive ? tt - 4 * h2 : 0u;
-                            if (nu1 > 15) continue;  // unreachable unless a state above is (then unsafe)
-                            pair_step[256 * q + 16 * c + nu0] = (uint8_t)((h1 + h2) | (nu1 << 2) | (alive << 6));
+                            const uint32_t nu1 = alive ? tt - 4 * h2 : NU_DEAD;
+                            if (alive && nu1 >= NU_DEAD) continue;  // unreachable unless a state above is (then unsafe)
+                            pair_step[256 * q + 16 * c + nu0] = (uint8_t)((h1 + h2) | (nu1 << 2));
                         }
                     }
                     std::map<uint32_t, double> next;
@@ -551,7 +553,7 @@ int build_image(const ksim_graph_desc *gs, int n_graphs, int F, HostImage &img, 
                     fs.swap(next);
                 }
                 for (const auto &sv : fs)
-                    if (sv.first > 15) pair_ok = false;
+                    if (sv.first >= NU_DEAD) pair_ok = false;
                 if (S > 0)
                     for (const auto &sv : fs) fast_max = std::max(fast_max, sv.second + std::log2(S) + 1e-12);
             }

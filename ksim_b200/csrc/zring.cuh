@@ -458,10 +458,12 @@ constexpr int TERM_FFK_BYTES = 128;
 // pairs with the factor 1, its sign bits being rows past the end, which are
 // zero): a table of the 16 products (4 x i8 each, combo c = pa | pb << 1 |
 // pa' << 2 | pb' << 3), then per pair a 256-byte step table: entry 16 c + nu,
-// for the valuation nu (0..15; a factor can have nu up to 6, so nu can grow,
-// and the packer sends terms that can leave that range to the exact path) of
-// z before the pair, holds the pair's halvings (bits 0-1), the valuation
-// after it (bits 2-5) and whether z stays nonzero (bit 6).
+// for the state nu of z before the pair — its valuation (0..14; a factor can
+// have nu up to 6, so nu can grow, and the packer sends terms that can leave
+// that range to the exact path) or NU_DEAD once z is zero (a class-0 kill or
+// a zero factor) — holds the pair's halvings (bits 0-1) and the state after
+// it (bits 2-5).  NU_DEAD absorbs and takes no halvings.
+constexpr uint32_t NU_DEAD = 15;
 // NodePhases products C lambda^e, e = -n1 .. n3, follow for terms with
 // class-1 or class-3 columns (n_cls[2], n_cls[3] in run order): 4 x u32 per
 // entry on the 32-bit NodePhases paths, 4 x u64 otherwise; entry i is
@@ -710,17 +712,15 @@ KS_HD const uint8_t *eval_term_rows(const uint8_t *p, const TermHdr &h, const Ro
         const uint8_t *pstep = p + term_pair_step_off(h);
         uint32_t nu[S];
 #pragma unroll
-        for (int s = 0; s < S; ++s) nu[s] = h.nu0;
+        for (int s = 0; s < S; ++s) nu[s] = alive[s] ? h.nu0 : NU_DEAD;  // a class-0 kill: no halvings
         for (uint32_t q = 0; q < n_pair; ++q) {
             const int pos = ph0 + 4 * (int)q;
 #pragma unroll
             for (int s = 0; s < S; ++s) {
                 const uint32_t c = (bits[s].word(pos >> 5) >> (pos & 31)) & 15u;
                 const uint32_t e = pstep[256 * q + 16 * c + nu[s]];
-                // a term already zero (class-0 kill, earlier zero factor) takes no halving
-                const uint32_t hh = e & 3u & (0u - alive[s]);
-                alive[s] &= e >> 6;
-                nu[s] = (e >> 2) & 15u;
+                const uint32_t hh = e & 3u;
+                nu[s] = e >> 2;
                 const uint32_t fw = *(const uint32_t *)(ptab + 64 * q + 4 * c);  // 4 x i8
                 const Zr<T> F = {(T)(int64_t)sext_byte<0>(fw), (T)(int64_t)sext_byte<1>(fw),
                                  (T)(int64_t)sext_byte<2>(fw), (T)(int64_t)sext_byte<3>(fw)};
