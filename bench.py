@@ -65,12 +65,12 @@ L2_FLUSH_BYTES = 256 << 20
 # k_sample on the same workload at 262,144 shots (dram__bytes_read.sum +
 # dram__bytes_write.sum), plus the output row the capture's L2 absorbed;
 # scaled to a launch by its shots.  Source: profiles/k_sample_cfg2_current.md.
-NCU_DRAM_BYTES_PER_SHOT = {"cfg2-medium-40q-t12": 67.6 + 40.0, "cfg4-large-rank-85q-t20": 61.2 + 16.0}
+NCU_DRAM_BYTES_PER_SHOT = {"cfg2-medium-40q-t12": 67.4 + 40.0, "cfg4-large-rank-85q-t20": 61.1 + 16.0}
 # Thread instructions per shot of the plain kernel on the same workload, from
 # one ncu capture (smsp__thread_inst_executed.sum / shots of the captured
 # launch); the issue roofline of the bench line is this times shots/s over
 # the SMs' issue ceiling.  Source: profiles/k_sample_cfg2_current.md.
-NCU_THREAD_INST_PER_SHOT = {"cfg2-medium-40q-t12": 155375, "cfg4-large-rank-85q-t20": 227680}
+NCU_THREAD_INST_PER_SHOT = {"cfg2-medium-40q-t12": 140295, "cfg4-large-rank-85q-t20": 205421}
 # Gate locations of the workloads' circuits (qubits x depth): one
 # single-qubit Pauli channel each in the noisy end-to-end leg.
 NOISE_LOCATIONS = {"cfg2-medium-40q-t12": 40 * 200, "cfg4-large-rank-85q-t20": 85 * 600}
