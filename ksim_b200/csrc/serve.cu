@@ -97,11 +97,12 @@ __device__ __forceinline__ T vload(const T *p)
     return *(const volatile T *)p;
 }
 
-// One tile of a job with the body compiled for the job's term paths, out of
-// line so each body keeps its own register allocation (the 32-bit and
-// hybrid bodies carry almost all work; the general one is rare).  Job data
-// comes through L2-only loads (CG): buffers are reused across requests
-// within one kernel lifetime.
+// One tile of a job with the body compiled for the job's W and term paths.
+// The loop inlines the bodies that carry most requests (all-32-bit W = 1
+// and 2, 32-bit and hybrid W = 2) and calls the others out of line (a call
+// costs the body about a tenth of its speed; inlining every body would
+// bloat the loop).  Job data comes through L2-only loads (CG): buffers are
+// reused across requests within one kernel lifetime.
 template <int W, int PATHS>
 __device__ __noinline__ bool serve_tile(const SampleJob &j, int64_t s0, uint64_t *bar, uint8_t *slots, uint32_t &g,
                                         uint8_t *scratch)
@@ -179,9 +180,18 @@ __global__ void __launch_bounds__(256, KSIM_SAMPLE_MIN_CTAS) k_serve(ServeJob *j
                  ? serve_tile<WW, PATHS_NARROW_HYBRID>(s_job, s0, bar, slots, g, scratch)              \
                  : serve_tile<WW, PATHS_ALL>(s_job, s0, bar, slots, g, scratch);                       \
         break;
+            // the common bodies inline, the rest out of line
+            if (s_W == 1 && paths == PATHS_NARROW)
+                ok = sample_tile<1, true, true, shots_per_thread(1), PATHS_NARROW>(s_job, s0, bar, slots, g, scratch);
+            else if (s_W == 2 && paths == PATHS_NARROW)
+                ok = sample_tile<2, true, true, shots_per_thread(2), PATHS_NARROW>(s_job, s0, bar, slots, g, scratch);
+            else if (s_W == 2 && paths == PATHS_NARROW_HYBRID)
+                ok = sample_tile<2, true, true, shots_per_thread(2), PATHS_NARROW_HYBRID>(s_job, s0, bar, slots, g, scratch);
+            else {
             switch (s_W) {
             KSIM_SERVE_W(1) KSIM_SERVE_W(2) KSIM_SERVE_W(3)
             default: KSIM_SERVE_W(4)
+            }
             }
 #undef KSIM_SERVE_W
             __threadfence();  // this thread's outputs before the counters below

@@ -153,6 +153,32 @@ def test_edge_cases_gpu(cuda_device, oracle_port):
         assert np.array_equal(bits, want[:, :4]) and same_bits(amp, wamp)
 
 
+@pytest.mark.parametrize("base", [-1060, -1022, -1005, 960, 1005])
+def test_scales_near_and_beyond_the_normal_range(cuda_device, oracle_port, base):
+    """power2 shifted by `base`: terms whose scales 2^(pw + power2) can reach
+    subnormal or infinite values take the general scale (pow2i), the others
+    the exponent-bits one (TF_EXP).  Per-term numerators, amplitudes and
+    sampled bits must be the oracle's on both sides of the boundary (at these
+    scales |A|^2 under- or overflows, so the bits degenerate as in the
+    reference; the shifts stop short of sums of opposite infinities, whose
+    NaN bit patterns differ between host and device)."""
+    rng = np.random.default_rng(1300 + abs(base))
+    comp = synth.random_component(rng, n_out=6, F=20, t=10, f_prob=0.1)
+    for g in comp.graphs:
+        g.pf_power2 = (g.pf_power2.astype(np.int64) + base).astype(np.int32)
+    kc = _component(comp.graphs, 20)
+    po = oracle_port.PortOracle(comp.graphs, 20)
+    for gi, g in enumerate(comp.graphs):
+        pv = rng.integers(0, 2, size=(128, g.np_params.shape[2])).astype(np.uint8)
+        assert np.array_equal(kc.eval_terms(gi, pv), po.eval_terms(gi, pv))
+        assert same_bits(kc.eval(gi, pv), po.eval(gi, pv))
+    f = synth.sample_f(rng, 3000, 20, 0.1)
+    for mode in (0, 1):
+        want, wamp = po.sample(f, 11, mode, return_amp=True)
+        bits, amp = device_sample(kc, f, 11, mode)
+        assert np.array_equal(bits, want[:, :6]) and same_bits(amp, wamp)
+
+
 def test_reference_api_edges(cuda_device):
     prog, _ = synth.htkh(1)
     graphs = prog.components[0].graphs
