@@ -88,16 +88,24 @@ ksim_status component_chunks(ksim_component *c, int slot_bytes, const ChunkDir *
 // After a synchronous call: KSIM_ERR_TIMEOUT if a staging wait of the
 // component's kernels ran out, clearing that flag (the other flags stay for
 // ksim_component_status).
+// A component's status word as read after a call (`flags`): a wait that
+// ran out fails the call and is cleared from the word (the other flags stay
+// for ksim_component_status).
+ksim_status report_timeout_flags(ksim_component *c, uint32_t flags)
+{
+    if (!(flags & KSIM_FLAG_WAIT_TIMEOUT)) return KSIM_OK;
+    const uint32_t rest = flags & ~(uint32_t)KSIM_FLAG_WAIT_TIMEOUT;
+    const cudaError_t e = cudaMemcpy(c->d_status, &rest, sizeof(rest), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "status write");
+    return fail(KSIM_ERR_TIMEOUT, "a staging wait of the sampling kernel ran out; its shots were not written");
+}
+
 ksim_status report_timeout(ksim_component *c)
 {
     uint32_t flags = 0;
     cudaError_t e = cudaMemcpy(&flags, c->d_status, sizeof(flags), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(e, "status read");
-    if (!(flags & KSIM_FLAG_WAIT_TIMEOUT)) return KSIM_OK;
-    const uint32_t rest = flags & ~(uint32_t)KSIM_FLAG_WAIT_TIMEOUT;
-    e = cudaMemcpy(c->d_status, &rest, sizeof(rest), cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) return cuda_fail(e, "status write");
-    return fail(KSIM_ERR_TIMEOUT, "a staging wait of the sampling kernel ran out; its shots were not written");
+    return report_timeout_flags(c, flags);
 }
 
 // Fill a SampleJob for component c; inputs/outputs set by the caller.
@@ -517,6 +525,11 @@ ksim_status ksim_program_create(ksim_component *const *comps, int32_t n_comps, c
             return cuda_fail(e, "cudaStreamCreate");
         }
     }
+    cudaError_t e = cudaMallocHost(&p->h_status, sizeof(uint32_t) * std::max<size_t>(p->parts.size(), 1));
+    if (e != cudaSuccess) {
+        ksim_program_destroy(p.release());
+        return cuda_fail(e, "cudaMallocHost(status words)");
+    }
     *out = p.release();
     return KSIM_OK;
 }
@@ -541,6 +554,7 @@ void ksim_program_destroy(ksim_program *p)
         if (st) cudaStreamDestroy(st);
     for (cudaEvent_t ev : p->ev_in) cudaEventDestroy(ev);
     for (cudaEvent_t ev : p->ev_done) cudaEventDestroy(ev);
+    if (p->h_status) cudaFreeHost(p->h_status);
     delete p;
 }
 
@@ -617,13 +631,17 @@ ksim_status ksim_program_sample_device(ksim_program *p, const uint8_t *d_f_param
 
 namespace {
 
-// Chunk boundaries of a host call over B shots.  Only the first chunk's
-// input copy and the last chunk's output copy are not hidden behind
-// sampling, so the chunks ramp: u, 2u, then chunks of about 4u, then 2u, u,
-// with u about B / 32 (at least 16 Ki shots, a multiple of 4 Ki).
-std::vector<int64_t> host_chunk_bounds(int64_t B)
+// Chunk boundaries of a host call over B shots whose rows move row_bytes
+// across PCIe (input and output together).  Only the first chunk's input
+// copy and the last chunk's output copy are not hidden behind sampling, so
+// the chunks ramp: u, 2u, then chunks of about 4u, then 2u, u, with u about
+// B / 32 shots — at least 16 Ki shots and 256 KiB of copies (a chunk costs
+// a few microseconds of launches and events, which a smaller copy does not
+// repay), a multiple of 4 Ki.
+std::vector<int64_t> host_chunk_bounds(int64_t B, int64_t row_bytes)
 {
-    const int64_t u = std::max<int64_t>((int64_t)1 << 14, (B / 32 + 4095) / 4096 * 4096);
+    const int64_t by_bytes = ((int64_t)1 << 18) / std::max<int64_t>(row_bytes, 1);
+    const int64_t u = (std::max<int64_t>({(int64_t)1 << 14, B / 32, by_bytes}) + 4095) / 4096 * 4096;
     std::vector<int64_t> b = {0};
     if (B <= 6 * u) {  // too few shots to ramp: chunks of u
         for (int64_t x = u; x < B; x += u) b.push_back(x);
@@ -677,7 +695,7 @@ ksim_status program_sample_host(ksim_program *p, const uint8_t *f, int64_t B, in
     uint8_t *d_in = packed ? (uint8_t *)p->ws_fp.p : d_f;       // where the host rows land
     uint8_t *d_back = packed ? (uint8_t *)p->ws_op.p : d_out;   // what goes back
 
-    const std::vector<int64_t> bounds = host_chunk_bounds(B);
+    const std::vector<int64_t> bounds = host_chunk_bounds(B, (noise ? 0 : f_row) + o_row);
     const int n_chunks = (int)bounds.size() - 1;
     std::vector<cudaEvent_t> &ev_in = p->ev_in, &ev_done = p->ev_done;
     ksim_status st = KSIM_OK;
@@ -723,6 +741,11 @@ ksim_status program_sample_host(ksim_program *p, const uint8_t *f, int64_t B, in
         if (e == cudaSuccess && i > 0) e = copy_back(i - 1);  // after chunk i is queued
     }
     if (e == cudaSuccess && st == KSIM_OK) e = copy_back(n_chunks - 1);
+    // the components' status words behind the last output copy (the output
+    // stream has waited for every chunk's sampling by then)
+    for (size_t k = 0; k < p->parts.size() && e == cudaSuccess && st == KSIM_OK; ++k)
+        e = cudaMemcpyAsync(p->h_status + k, p->parts[k].comp->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                            p->s_d2h);
     if (e == cudaSuccess && st == KSIM_OK) {
         // every chunk's output copy waited for its sampling, which waited for
         // its input copy: the output stream's end is the call's end
@@ -735,8 +758,8 @@ ksim_status program_sample_host(ksim_program *p, const uint8_t *f, int64_t B, in
     if (st != KSIM_OK) return st;
     if (e != cudaSuccess) return cuda_fail(e, "program sample");
     ksim_status rep = KSIM_OK;
-    for (auto &part : p->parts) {
-        const ksim_status r = report_timeout(part.comp);
+    for (size_t k = 0; k < p->parts.size(); ++k) {
+        const ksim_status r = report_timeout_flags(p->parts[k].comp, p->h_status[k]);
         if (rep == KSIM_OK) rep = r;
     }
     return rep;

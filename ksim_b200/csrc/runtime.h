@@ -74,6 +74,7 @@ struct ksim_program {
     // (consecutive chunks overlap) and one stream per copy direction
     cudaStream_t cs[KSIM_HOST_STREAMS] = {}, s_h2d = nullptr, s_d2h = nullptr;
     std::vector<cudaEvent_t> ev_in, ev_done;  // per chunk, kept across calls
+    uint32_t *h_status = nullptr;             // page-locked: the components' status words after a call
     ksim::DevBuf ws_f, ws_out, ws_fp, ws_op;  // unpacked rows; bit-packed rows
     std::mutex mu;
 };

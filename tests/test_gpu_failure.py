@@ -61,6 +61,24 @@ def test_plain_wait_timeout_is_reported_and_context_survives(cuda_device, oracle
     assert kc.status() == 0
 
 
+def test_program_call_reports_a_wait_timeout(cuda_device, oracle_port):
+    """The pipelined host call of a program reads its components' status
+    words behind its last output copy: a wait that ran out fails the call
+    (and leaves the word clear), and the next call is exact."""
+    from ksim_b200._abi import FLAG_WAIT_TIMEOUT
+    from ksim_b200.sampler import B200ProgramSampler
+    comp, _, f = _component()
+    prog = synth.single_component_program(comp)
+    s = B200ProgramSampler(prog, device=0)
+    kc = s.components[0][1]
+    kc.set_wait_limit(1)
+    with pytest.raises(TimeoutError, match="staging wait"):
+        s.sample(f, 5)
+    assert not kc.status() & FLAG_WAIT_TIMEOUT
+    kc.set_wait_limit(0)
+    assert np.array_equal(s.sample(f, 5), oracle_port.program_sample(prog, f, 5))
+
+
 def test_served_wait_timeout_fails_the_request_only(cuda_device, oracle_port):
     from ksim_b200.serve import Server
     comp, _, f = _component(911)

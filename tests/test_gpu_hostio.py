@@ -40,11 +40,11 @@ def _device_once(sampler, f, seed, mode):
     return d_out.cpu().numpy()
 
 
-def _chunk_bounds(B):
+def _chunk_bounds(B, row_bytes):
     """The host call's chunk schedule (api.cu host_chunk_bounds): u, 2u,
-    chunks of about 4u, 2u, u with u ~ B / 32 (>= 16 Ki, a multiple of 4 Ki),
-    or chunks of u when B <= 6u."""
-    u = max(1 << 14, (B // 32 + 4095) // 4096 * 4096)
+    chunks of about 4u, 2u, u with u ~ B / 32 (>= 16 Ki shots and 256 KiB of
+    copies, a multiple of 4 Ki), or chunks of u when B <= 6u."""
+    u = (max(1 << 14, B // 32, (1 << 18) // max(row_bytes, 1)) + 4095) // 4096 * 4096
     if B <= 6 * u:
         return list(range(0, B, u)) + [B]
     body = B - 6 * u
@@ -63,7 +63,7 @@ def test_chunked_host_call_equals_one_launch(cuda_device, oracle_port, small_pro
         got = s.sample(f, 31 + B, rng_mode=mode)
         assert np.array_equal(got, _device_once(s, f, 31 + B, mode)), mode
     # spot-check against the oracle across the chunk seams
-    bounds = _chunk_bounds(B)
+    bounds = _chunk_bounds(B, f.shape[1] + s.num_outputs)
     assert all(x < y for x, y in zip(bounds, bounds[1:])) and bounds[-1] == B
     got = s.sample(f, 31 + B, rng_mode=1)
     for lo in sorted({max(0, x - 150) for x in bounds}):
