@@ -116,7 +116,10 @@ int64_t ksim_component_image_bytes(const ksim_component *c);
 
 /* Host buffers, synchronous.  f_sel: (B, num_f) uint8 C-contiguous; out:
  * (B, max(n_out,1)) uint8.  Replaces Component.sample, kokkos_sim.cpp:188-241
- * (bit-identical to it with rng_mode = KSIM_RNG_XORSHIFT). */
+ * (bit-identical to it with rng_mode = KSIM_RNG_XORSHIFT).  Runs as the
+ * pipelined host call of ksim_program_sample on the component alone (built
+ * on the first call, freed with the component), so copies overlap sampling;
+ * page-locked buffers overlap best. */
 ksim_status ksim_component_sample(ksim_component *c, const uint8_t *f_sel, int64_t B,
                                   uint64_t seed, int32_t rng_mode, uint8_t *out);
 

@@ -7,8 +7,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <map>
 #include <mutex>
+#include <numeric>
 #include <string>
 #include <vector>
 
@@ -131,6 +133,13 @@ ksim_status component_job(ksim_component *c, const LaunchCfg &cfg, SampleJob &j)
 
 }  // namespace ksim
 
+namespace {
+// Host buffers in and out of a program, chunked and copy-overlapped (below).
+ksim_status program_sample_host(ksim_program *p, const uint8_t *f, int64_t B, int64_t n_f_cols, uint64_t seed,
+                                int32_t rng_mode, uint8_t *out, bool packed, const ksim_noise *noise = nullptr,
+                                uint64_t noise_seed = 0);
+}  // namespace
+
 using namespace ksim;
 
 extern "C" {
@@ -216,6 +225,7 @@ void ksim_component_destroy(ksim_component *c)
 {
     if (!c) return;
     DeviceGuard g(c->device);
+    if (c->self_prog) ksim_program_destroy(c->self_prog);
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (auto &kv : c->chunks) cudaFree(kv.second.d);
     c->ws_f.release();
@@ -341,41 +351,32 @@ ksim_status ksim_component_sample(ksim_component *c, const uint8_t *f_sel, int64
     if (B < 0) return fail(KSIM_ERR_INVALID_ARGUMENT, "B must be >= 0");
     if (check_rng(rng_mode) != KSIM_OK) return KSIM_ERR_INVALID_ARGUMENT;
     const int F = c->img.F, n_out = c->img.n_out;
-    const int64_t ncol = std::max(n_out, 1);
     if (B == 0) return KSIM_OK;
     if ((F > 0 && !f_sel) || !out) return fail(KSIM_ERR_INVALID_ARGUMENT, "input or output pointer is NULL");
-    DeviceGuard g(c->device);
-    std::lock_guard<std::mutex> lk(c->mu);
-    cudaError_t e = c->ws_f.ensure((size_t)std::max<int64_t>(B * F, 1));
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(f workspace)");
-    e = c->ws_out.ensure((size_t)(B * ncol));
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(output workspace)");
-    if (F > 0) {
-        e = cudaMemcpyAsync(c->ws_f.p, f_sel, (size_t)(B * F), cudaMemcpyHostToDevice, c->stream);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync(f)");
+    if (n_out == 0) {  // the reference pads its output to one zero column (kokkos_sim.cpp:233-240)
+        std::memset(out, 0, (size_t)B);
+        return KSIM_OK;
     }
-    if (n_out == 0) {
-        e = cudaMemsetAsync(c->ws_out.p, 0, (size_t)(B * ncol), c->stream);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(out)");
-    } else {
-        SampleJob j = {};
-        ksim_status st = component_job(c, c->cfg, j);
-        if (st != KSIM_OK) return st;
-        j.rng_mode = rng_mode;
-        j.f = (const uint8_t *)c->ws_f.p;
-        j.f_stride = F;
-        j.out = (uint8_t *)c->ws_out.p;
-        j.out_stride = ncol;
-        j.B = B;
-        j.seed = seed;
-        e = launch_sample(j, c->img.W, c->cfg, c->stream);
-        if (e != cudaSuccess) return cuda_fail(e, "sample kernel launch");
+    // the pipelined host call of the component alone as a program: identity
+    // f_selection and output order, component seed offset 0, so the bits are
+    // this component's
+    ksim_program *p = nullptr;
+    {
+        DeviceGuard g(c->device);
+        std::lock_guard<std::mutex> lk(c->mu);
+        if (!c->self_prog) {
+            std::vector<int32_t> sel((size_t)F), order((size_t)n_out);
+            std::iota(sel.begin(), sel.end(), 0);
+            std::iota(order.begin(), order.end(), 0);
+            ksim_component *comps[1] = {c};
+            const int32_t *sels[1] = {sel.data()};
+            const int32_t lens[1] = {F};
+            const ksim_status st = ksim_program_create(comps, 1, sels, lens, order.data(), n_out, &c->self_prog);
+            if (st != KSIM_OK) return st;
+        }
+        p = c->self_prog;
     }
-    e = cudaMemcpyAsync(out, c->ws_out.p, (size_t)(B * ncol), cudaMemcpyDeviceToHost, c->stream);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync(out)");
-    e = cudaStreamSynchronize(c->stream);
-    if (e != cudaSuccess) return cuda_fail(e, "sample");
-    return report_timeout(c);
+    return program_sample_host(p, f_sel, B, F, seed, rng_mode, out, false);
 }
 
 static ksim_status eval_common(ksim_component *c, int32_t graph, const uint8_t *params, int64_t B, int64_t P,
@@ -670,8 +671,8 @@ std::vector<int64_t> host_chunk_bounds(int64_t B, int64_t row_bytes)
 // noise (nullable): f rows are drawn on the device from this model with
 // noise_seed instead of being copied from `f`.
 ksim_status program_sample_host(ksim_program *p, const uint8_t *f, int64_t B, int64_t n_f_cols, uint64_t seed,
-                                int32_t rng_mode, uint8_t *out, bool packed, const ksim_noise *noise = nullptr,
-                                uint64_t noise_seed = 0)
+                                int32_t rng_mode, uint8_t *out, bool packed, const ksim_noise *noise,
+                                uint64_t noise_seed)
 {
     if (!p) return fail(KSIM_ERR_INVALID_ARGUMENT, "program is NULL");
     if (B < 0 || n_f_cols < 0) return fail(KSIM_ERR_INVALID_ARGUMENT, "B and n_f_cols must be >= 0");

@@ -51,7 +51,8 @@ struct ksim_component {
     ksim::DevBuf ws_f, ws_out, ws_aux;
     ksim::LaunchCfg cfg;
     int64_t wait_limit = 0;  // polls of a staging wait (0: the kernels' default)
-    std::mutex mu;        // workspaces and cfg
+    ksim_program *self_prog = nullptr;  // this component alone as a program (host-buffer sample calls)
+    std::mutex mu;        // workspaces, cfg and self_prog
     std::mutex chunk_mu;  // the chunk-directory map
 };
 
