@@ -70,7 +70,7 @@ NCU_DRAM_BYTES_PER_SHOT = {"cfg2-medium-40q-t12": 67.4 + 40.0, "cfg4-large-rank-
 # one ncu capture (smsp__thread_inst_executed.sum / shots of the captured
 # launch); the issue roofline of the bench line is this times shots/s over
 # the SMs' issue ceiling.  Source: profiles/k_sample_cfg2_current.md.
-NCU_THREAD_INST_PER_SHOT = {"cfg2-medium-40q-t12": 140295, "cfg4-large-rank-85q-t20": 205421}
+NCU_THREAD_INST_PER_SHOT = {"cfg2-medium-40q-t12": 138386, "cfg4-large-rank-85q-t20": 201817}
 # Gate locations of the workloads' circuits (qubits x depth): one
 # single-qubit Pauli channel each in the noisy end-to-end leg.
 NOISE_LOCATIONS = {"cfg2-medium-40q-t12": 40 * 200, "cfg4-large-rank-85q-t20": 85 * 600}

@@ -206,8 +206,10 @@ ksim_status ksim_component_create(const ksim_graph_desc *graphs, int32_t n_graph
     // staging is skipped when two slots would not fit in shared memory
     c->cfg.paths = c->img.n_narrow_terms == c->img.n_terms ? 1
                    : c->img.n_narrow_terms + c->img.n_hybrid_terms == c->img.n_terms ? 2 : 0;
-    // 12 KiB slots for the specialised kernels (five CTAs per SM), 16 KiB else
-    const int64_t slot = std::max<int64_t>(c->cfg.paths != 0 ? 12288 : 16384,
+    // slots for the specialised kernels as large as five CTAs per SM allow
+    // (14 KiB for W <= 2, 12 KiB for W = 3, 4: fewer chunks per graph), 16 KiB
+    // else
+    const int64_t slot = std::max<int64_t>(c->cfg.paths != 0 ? (c->img.W <= 2 ? 14336 : 12288) : 16384,
                                            (c->img.max_term_bytes + 15) & ~int64_t(15));
     c->cfg.threads = 128;  // CTAs of 128: a quarter of the warps per barrier
     c->cfg.slot_bytes = (int)std::min<int64_t>(slot, 1 << 30);

@@ -287,7 +287,7 @@ __device__ __forceinline__ const uint8_t *eval_terms_warp(const uint8_t *p, uint
                 const uint32_t n_pairs = m.n_pairs;
                 const uint32_t *ix = (const uint32_t *)(blk + BLOCK_HEAD_BYTES) + lane;
                 uint64_t acc = 0;
-#pragma unroll 2
+#pragma unroll 4
                 for (uint32_t i = 0; i < n_pairs; ++i) {
                     const uint32_t x = ix[32 * i];
                     acc ^= *(const uint64_t *)(sw + (x & 0xFFFFu)) ^ *(const uint64_t *)(sw + (x >> 16));
