@@ -21,11 +21,14 @@
 //     (until it reaches 0 or the run's length).
 // On the device one thread owns one shot and, per run, jumps from firing
 // channel to firing channel: from position j the next firing channel is
-// j + 1 + #{k : u < T_k} for a fresh 32-bit draw u (binary search in the
-// decreasing table), since P(no fire in the next k channels) = (1 - p)^k;
-// an outcome is then the first whose conditional-CDF threshold exceeds a
-// second draw, and its f pattern is XORed in.  Work per shot is proportional
-// to the channels that fire, not to the channels of the model.  The draws
+// j + 1 + #{k : u < T_k} for a fresh 32-bit draw u, since P(no fire in the
+// next k channels) = (1 - p)^k: the count starts from the logarithm's guess
+// log2(u 2^-32) / log2(1 - p) and one or two table reads make it exact (the
+// walks from the guess end at the count whatever the guess); an outcome is
+// then the first whose conditional-CDF threshold exceeds a second draw, and
+// its f pattern is XORed in.  Work per shot is proportional to the channels
+// that fire, not to the channels of the model.  Rows are written as 16-byte
+// pieces of 0/1 bytes where they start on 16-byte boundaries.  The draws
 // are one counter-based Philox4x32-10 stream per shot (key = seed, counter =
 // (shot, block, 0, tag), four draws a block, consumed in order), so any shot
 // range can be drawn alone and the oracle's CPU restatement reproduces every
@@ -63,6 +66,8 @@ struct NoiseRun {
     uint32_t n;         // channels in the run
     uint32_t skip_off;  // its skip table T_1.. in the skip array
     uint32_t skip_len;
+    float inv_log2q;    // 1 / log2(1 - p): the skip's first guess
+    uint32_t pad[3];
 };
 
 constexpr uint32_t NOISE_TAG = 0x4E4F4953u;
@@ -93,7 +98,7 @@ __global__ void __launch_bounds__(256) k_noise(const NoiseRun *__restrict__ runs
                                                const NoiseChan *__restrict__ ch, const uint32_t *__restrict__ cdf,
                                                const uint64_t *__restrict__ pat, const uint32_t *__restrict__ skip,
                                                int num_f, int64_t B, int64_t shot_offset, uint64_t seed,
-                                               uint8_t *__restrict__ f, int64_t f_stride)
+                                               uint8_t *__restrict__ f, int64_t f_stride, bool vec_rows)
 {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= B) return;
@@ -110,15 +115,17 @@ __global__ void __launch_bounds__(256) k_noise(const NoiseRun *__restrict__ runs
         const uint32_t *T = skip + R.skip_off;
         int64_t j = -1;  // last channel of the run visited
         for (;;) {
-            // k* = #{k in 1..skip_len : u < T_k}: T decreasing, binary search
+            // k* = #{k in 1..skip_len : u < T_k}, T decreasing: the first
+            // index i of T (T[i] = T_{i+1}) with u >= T[i], or skip_len.
+            // First guess from u < (1 - p)^k 2^32 <=> k < log2(u 2^-32) /
+            // log2(1 - p); the two walks then make it exact whatever the
+            // guess (within one or two of k* here, so a table read or two)
             const uint32_t u = st.next();
-            uint32_t lo = 0, hi = R.skip_len;
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi + 1) >> 1;
-                if (u < __ldg(T + mid - 1)) lo = mid;
-                else hi = mid - 1;
-            }
-            j += (int64_t)lo + 1;  // every step advances: at most n steps per run
+            const float g = (__log2f((float)u + 0.5f) - 32.0f) * R.inv_log2q;
+            uint32_t k = g <= 0.0f ? 0u : g >= (float)R.skip_len ? R.skip_len : (uint32_t)g;
+            while (k < R.skip_len && u < __ldg(T + k)) ++k;
+            while (k > 0 && u >= __ldg(T + k - 1)) --k;
+            j += (int64_t)k + 1;  // every step advances: at most n steps per run
             if (j >= (int64_t)R.n) break;
             const NoiseChan c = ch[R.first + (uint32_t)j];
             const uint32_t v = st.next();
@@ -130,10 +137,24 @@ __global__ void __launch_bounds__(256) k_noise(const NoiseRun *__restrict__ runs
         }
     }
     uint8_t *row = f + s * f_stride;
+    // 16-byte rows of 0/1 bytes where the rows allow it: a nibble n spreads
+    // to four bytes as (n * 0x00204081) & 0x01010101 (its copies shifted by
+    // 0, 7, 14, 21 do not overlap, and byte k keeps bit k)
+    const int vec16 = vec_rows ? num_f >> 4 : 0;
 #pragma unroll
     for (int w = 0; w < W; ++w) {  // static word indices keep acc in registers
+        const int q0 = 4 * w, q1 = min(4 * w + 4, vec16);
+        for (int q = q0; q < q1; ++q) {
+            const uint32_t h = (uint32_t)(acc[w] >> (16 * (q - q0)));
+            uint4 v;
+            v.x = ((h & 0xFu) * 0x00204081u) & 0x01010101u;
+            v.y = (((h >> 4) & 0xFu) * 0x00204081u) & 0x01010101u;
+            v.z = (((h >> 8) & 0xFu) * 0x00204081u) & 0x01010101u;
+            v.w = (((h >> 12) & 0xFu) * 0x00204081u) & 0x01010101u;
+            *(uint4 *)(row + 16 * q) = v;
+        }
         const int lim = min(64, num_f - 64 * w);
-        for (int b = 0; b < lim; ++b) row[64 * w + b] = (uint8_t)((acc[w] >> b) & 1u);
+        for (int b = max(16 * (q1 - q0), 0); b < lim; ++b) row[64 * w + b] = (uint8_t)((acc[w] >> b) & 1u);
     }
 }
 
@@ -168,8 +189,10 @@ cudaError_t launch_noise_w(const ksim_noise *n, int64_t B, int64_t shot_offset, 
 {
     const int64_t blocks = (B + 255) / 256;
     if (blocks > 0x7FFFFFFF) return cudaErrorInvalidConfiguration;
+    // rows start on 16-byte boundaries: whole 16-byte pieces are stored at once
+    const bool vec_rows = ((uintptr_t)f & 15u) == 0 && (f_stride & 15) == 0;
     k_noise<W><<<(unsigned)blocks, 256, 0, st>>>(n->d_runs, n->n_runs, n->d_ch, n->d_cdf, n->d_pat, n->d_skip,
-                                                 n->num_f, B, shot_offset, seed, f, f_stride);
+                                                 n->num_f, B, shot_offset, seed, f, f_stride, vec_rows);
     return cudaGetLastError();
 }
 
@@ -329,6 +352,8 @@ ksim_status ksim_noise_create(const double *probs, const int32_t *n_bits, int32_
             skip.push_back(thr);
         }
         run.skip_len = (uint32_t)skip.size() - run.skip_off;
+        run.inv_log2q = q > 0.0 ? (float)(1.0 / std::log2(q)) : 0.0f;
+        run.pad[0] = run.pad[1] = run.pad[2] = 0;
         runs.push_back(run);
         for (size_t x = r0; x < r1; ++x) {
             const HostChan &hc = merged[order[x]];

@@ -27,7 +27,7 @@ def _model(seed, num_f=40, n_ch=60):
     return probs, T
 
 
-@pytest.mark.parametrize("num_f", [0, 7, 64, 65, 130])
+@pytest.mark.parametrize("num_f", [0, 7, 64, 65, 96, 130, 144])
 def test_device_draw_equals_oracle(cuda_device, oracle_port, num_f):
     from ksim_b200.noise import DeviceChannelSampler
     probs, T = _model(num_f, num_f=num_f)
