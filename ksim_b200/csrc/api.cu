@@ -528,6 +528,9 @@ ksim_status ksim_program_create(ksim_component *const *comps, int32_t n_comps, c
             return cuda_fail(e, "cudaStreamCreate");
         }
     }
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device);
+    p->wave_shots = (int64_t)std::max(sms, 1) * 5 * 256;  // five CTAs of 256 shots per SM
     cudaError_t e = cudaMallocHost(&p->h_status, sizeof(uint32_t) * std::max<size_t>(p->parts.size(), 1));
     if (e != cudaSuccess) {
         ksim_program_destroy(p.release());
@@ -665,8 +668,8 @@ std::vector<int64_t> host_chunk_bounds(int64_t B, int64_t row_bytes)
 // Host buffers in, host buffers out, in chunks of shots (host_chunk_bounds)
 // pipelined over copy and compute streams: the f rows of chunk i+1 cross
 // PCIe while chunk i samples, the results of chunk i cross back while later
-// chunks sample, and consecutive chunks take the compute streams in turn so
-// their waves of CTAs overlap.  Chunk c samples with shot_offset = its first
+// chunks sample (page-locked buffers), and consecutive chunks take the
+// compute streams in turn so their waves of CTAs overlap.  Chunk c samples with shot_offset = its first
 // row, so the bits equal a single launch over all B shots.
 // packed: f rows of ceil(n_f_cols/8) bytes and output rows of
 // ceil(n_outputs/8) bytes, bit c of a row in byte c/8 at bit c%8.
@@ -700,6 +703,9 @@ ksim_status program_sample_host(ksim_program *p, const uint8_t *f, int64_t B, in
 
     const std::vector<int64_t> bounds = host_chunk_bounds(B, (noise ? 0 : f_row) + o_row);
     const int n_chunks = (int)bounds.size() - 1;
+    int64_t largest = 1;
+    for (int i = 0; i < n_chunks; ++i) largest = std::max(largest, bounds[i + 1] - bounds[i]);
+    const int lag = (int)std::min<int64_t>(KSIM_HOST_STREAMS, std::max<int64_t>(1, (p->wave_shots + largest - 1) / largest));
     std::vector<cudaEvent_t> &ev_in = p->ev_in, &ev_done = p->ev_done;
     ksim_status st = KSIM_OK;
     while ((int)ev_in.size() < n_chunks && e == cudaSuccess) {
@@ -741,9 +747,16 @@ ksim_status program_sample_host(ksim_program *p, const uint8_t *f, int64_t B, in
         if (st != KSIM_OK) break;
         if (packed) e = launch_pack_bits(d_out + c0 * n_out, n, n_out, o_row, d_back + c0 * o_row, cs);
         if (e == cudaSuccess) e = cudaEventRecord(ev_done[i], cs);
-        if (e == cudaSuccess && i > 0) e = copy_back(i - 1);  // after chunk i is queued
+        // chunk i - lag's output copy once chunk i is queued: into
+        // page-locked memory copies are asynchronous and start as each chunk
+        // ends; into pageable memory each one holds the host until it is
+        // done, so the lag keeps about a wave of CTAs queued meanwhile (small
+        // chunks: up to one per compute stream) without leaving more than
+        // that many copies for after the last chunk
+        if (e == cudaSuccess && i >= lag) e = copy_back(i - lag);
     }
-    if (e == cudaSuccess && st == KSIM_OK) e = copy_back(n_chunks - 1);
+    for (int i = std::max(0, n_chunks - lag); i < n_chunks && e == cudaSuccess && st == KSIM_OK; ++i)
+        e = copy_back(i);
     // the components' status words behind the last output copy (the output
     // stream has waited for every chunk's sampling by then)
     for (size_t k = 0; k < p->parts.size() && e == cudaSuccess && st == KSIM_OK; ++k)

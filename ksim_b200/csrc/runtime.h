@@ -76,6 +76,7 @@ struct ksim_program {
     cudaStream_t cs[KSIM_HOST_STREAMS] = {}, s_h2d = nullptr, s_d2h = nullptr;
     std::vector<cudaEvent_t> ev_in, ev_done;  // per chunk, kept across calls
     uint32_t *h_status = nullptr;             // page-locked: the components' status words after a call
+    int64_t wave_shots = 1;                   // shots one wave of sampling CTAs holds on the device
     ksim::DevBuf ws_f, ws_out, ws_fp, ws_op;  // unpacked rows; bit-packed rows
     std::mutex mu;
 };
