@@ -33,6 +33,19 @@ def _check_component(hostemu, oracle_port, comp, F, rng, B=128):
     return he.stats()
 
 
+@pytest.mark.parametrize("base", [-1060, -1022, -1005, 960, 1005])
+def test_scales_near_and_beyond_the_normal_range(hostemu, oracle_port, base):
+    """power2 shifted by `base`: terms whose scales 2^(pw + power2) can be
+    subnormal or infinite take pow2i, the others the exponent-bits scale
+    (TF_EXP); both must give the oracle's doubles (shifts short of sums of
+    opposite infinities, whose NaN bit patterns need not agree)."""
+    rng = np.random.default_rng(2600 + abs(base))
+    comp = synth.random_component(rng, n_out=5, F=16, t=9, f_prob=0.1)
+    for g in comp.graphs:
+        g.pf_power2 = (g.pf_power2.astype(np.int64) + base).astype(np.int32)
+    _check_component(hostemu, oracle_port, comp, 16, rng)
+
+
 @pytest.mark.parametrize("seed", range(10))
 def test_random_components(hostemu, oracle_port, seed):
     rng = np.random.default_rng(seed)
