@@ -64,12 +64,14 @@ L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes per shot of the plain kernel, from one ncu capture of
 # k_sample on the same workload at 262,144 shots (dram__bytes_read.sum +
 # dram__bytes_write.sum), plus the output row the capture's L2 absorbed;
-# scaled to a launch by its shots.  Source: profiles/k_sample_cfg2_current.md.
+# scaled to a launch by its shots (the capture's command and figures are kept
+# with the ncu summaries under profiles/).
 NCU_DRAM_BYTES_PER_SHOT = {"cfg2-medium-40q-t12": 67.4 + 40.0, "cfg4-large-rank-85q-t20": 61.1 + 16.0}
 # Thread instructions per shot of the plain kernel on the same workload, from
 # one ncu capture (smsp__thread_inst_executed.sum / shots of the captured
 # launch); the issue roofline of the bench line is this times shots/s over
-# the SMs' issue ceiling.  Source: profiles/k_sample_cfg2_current.md.
+# the SMs' issue ceiling (capture command and figures: the ncu summaries
+# under profiles/).
 NCU_THREAD_INST_PER_SHOT = {"cfg2-medium-40q-t12": 138386, "cfg4-large-rank-85q-t20": 201817}
 # Gate locations of the workloads' circuits (qubits x depth): one
 # single-qubit Pauli channel each in the noisy end-to-end leg.
@@ -768,7 +770,7 @@ def main():
             "issue_frac": issue / issue_peak if issue else None,
             "inst_per_shot": inst,
             "inst_source": "ncu smsp__thread_inst_executed.sum of k_sample on this workload / shots "
-                           "(profiles/k_sample_cfg2_current.md)",
+                           "(one capture of 262,144 shots; summary under profiles/)",
             "peak_source": f"{sms} SMs x 4 issue slots x 32 lanes x median sampled SM clock "
                            f"({sm_mhz:.0f} MHz)",
             "ops_per_shot": work["ops"],

@@ -2,8 +2,8 @@
 
 Runs only where the reference checkout is available (KSIM_REF_TREE).  The
 reference's ``sample/sampler.py`` is imported unmodified with
-``sys.modules["kokkos_sim"] = ksim_b200.kokkos_sim``, the switch INTEGRATION.md
-describes.  On a machine without a GPU the native Component cannot upload, so
+``sys.modules["kokkos_sim"] = ksim_b200.kokkos_sim`` (the one-line switch a
+maintainer makes to run the reference's caller on this package).  On a machine without a GPU the native Component cannot upload, so
 this checks the contract up to the device: the reference constructs
 ``Component(graphs, num_f)`` with the dicts of its ``_graph_to_dict``
 (sampler.py:21-43), those dicts are byte-identical to this package's
