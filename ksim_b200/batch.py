@@ -1,10 +1,13 @@
-"""Batched sampling: many FlatPrograms in one persistent, graph-captured launch.
+"""Batched sampling: many FlatPrograms in one graph-captured launch.
 
 ``BatchSampler(programs, shots)`` uploads every program once, keeps one device
 input buffer (the full f matrix) and one device output buffer per program,
 and turns every component of every program into a job of one
 ``ksim_batch`` (``include/ksim_b200.h``): longest-first work items pulled by
-persistent CTAs, the launch captured in a CUDA graph and replayed.  Each
+persistent CTAs, one kernel per (W, term paths) class of jobs, the class
+kernels chained on one stream as programmatic dependent launches (each
+starts while the one before it drains), all captured in a CUDA graph and
+replayed.  Each
 program's result is bit-identical to ``B200ProgramSampler(prog).sample``
 with the same seed — shot s of a job always uses stream index s, whatever
 else shares the launch.
@@ -64,7 +67,7 @@ def _store_cache(key: str, value: dict) -> None:
 
 
 class BatchSampler:
-    """Sample several FlatPrograms in one launch.
+    """Sample several FlatPrograms in one graph launch.
 
     ``programs``: list of FlatProgram; ``shots``: shots per program.
     Inputs come from host arrays (``set_inputs``) or stay on the device
