@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/ksim_b200.h"
+#include "hostio.h"
 #include "image.h"
 #include "kernels.h"
 #include "runtime.h"
@@ -637,34 +638,6 @@ ksim_status ksim_program_sample_device(ksim_program *p, const uint8_t *d_f_param
 
 namespace {
 
-// Chunk boundaries of a host call over B shots whose rows move row_bytes
-// across PCIe (input and output together).  Only the first chunk's input
-// copy and the last chunk's output copy are not hidden behind sampling, so
-// the chunks ramp: u, 2u, then chunks of about 4u, then 2u, u, with u about
-// B / 32 shots — at least 16 Ki shots and 256 KiB of copies (a chunk costs
-// a few microseconds of launches and events, which a smaller copy does not
-// repay), a multiple of 4 Ki.
-std::vector<int64_t> host_chunk_bounds(int64_t B, int64_t row_bytes)
-{
-    const int64_t by_bytes = ((int64_t)1 << 18) / std::max<int64_t>(row_bytes, 1);
-    const int64_t u = (std::max<int64_t>({(int64_t)1 << 14, B / 32, by_bytes}) + 4095) / 4096 * 4096;
-    std::vector<int64_t> b = {0};
-    if (B <= 6 * u) {  // too few shots to ramp: chunks of u
-        for (int64_t x = u; x < B; x += u) b.push_back(x);
-        b.push_back(B);
-        return b;
-    }
-    b.push_back(u);
-    b.push_back(3 * u);
-    const int64_t body = B - 6 * u, n_body = (body + 4 * u - 1) / (4 * u);
-    const int64_t step = (body / n_body + 4095) / 4096 * 4096;
-    for (int64_t k = 1; k < n_body; ++k) b.push_back(3 * u + k * step);
-    b.push_back(B - 3 * u);
-    b.push_back(B - u);
-    b.push_back(B);
-    return b;
-}
-
 // Host buffers in, host buffers out, in chunks of shots (host_chunk_bounds)
 // pipelined over copy and compute streams: the f rows of chunk i+1 cross
 // PCIe while chunk i samples, the results of chunk i cross back while later
@@ -703,9 +676,7 @@ ksim_status program_sample_host(ksim_program *p, const uint8_t *f, int64_t B, in
 
     const std::vector<int64_t> bounds = host_chunk_bounds(B, (noise ? 0 : f_row) + o_row);
     const int n_chunks = (int)bounds.size() - 1;
-    int64_t largest = 1;
-    for (int i = 0; i < n_chunks; ++i) largest = std::max(largest, bounds[i + 1] - bounds[i]);
-    const int lag = (int)std::min<int64_t>(KSIM_HOST_STREAMS, std::max<int64_t>(1, (p->wave_shots + largest - 1) / largest));
+    const int lag = host_copy_lag(bounds, p->wave_shots, KSIM_HOST_STREAMS);
     std::vector<cudaEvent_t> &ev_in = p->ev_in, &ev_done = p->ev_done;
     ksim_status st = KSIM_OK;
     while ((int)ev_in.size() < n_chunks && e == cudaSuccess) {

@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "hostio.h"
 #include "image.h"
 #include "serve_sched.h"
 #include "zring.cuh"
@@ -233,6 +234,20 @@ int hostemu_admissible(int64_t need_bytes, int need_jobs, int64_t need_ring, int
     const AdmitNeed n = {need_bytes, need_jobs, need_ring};
     const AdmitState st = {&a, &rq, &jb, ring_cap, ring_in_flight};
     return admissible(n, st);
+}
+
+// The chunk plan of a host-buffer call (hostio.h): boundaries into out (at
+// most cap), returns their count.
+int hostemu_chunk_bounds(int64_t B, int64_t row_bytes, int64_t *out, int cap)
+{
+    const std::vector<int64_t> b = ksim::host_chunk_bounds(B, row_bytes);
+    for (size_t i = 0; i < b.size() && (int)i < cap; ++i) out[i] = b[i];
+    return (int)b.size();
+}
+
+int hostemu_copy_lag(const int64_t *bounds, int n, int64_t wave_shots, int max_lag)
+{
+    return ksim::host_copy_lag(std::vector<int64_t>(bounds, bounds + n), wave_shots, max_lag);
 }
 
 }  // extern "C"
