@@ -73,6 +73,12 @@ NCU_DRAM_BYTES_PER_SHOT = {"cfg2-medium-40q-t12": 67.4 + 40.0, "cfg4-large-rank-
 # the SMs' issue ceiling (capture command and figures: the ncu summaries
 # under profiles/).
 NCU_THREAD_INST_PER_SHOT = {"cfg2-medium-40q-t12": 138386, "cfg4-large-rank-85q-t20": 201817}
+# Thread instructions of one cfg3 batch (its five class kernels, one ncu
+# capture at the default launch shape: 128 threads, 14 KiB slots); the
+# batched leg's issue fraction is this over its timed batch and the issue
+# ceiling (capture command and figures: the ncu summaries under profiles/).
+NCU_THREAD_INST_PER_BATCH = 88.83e9
+NCU_BATCH_SHAPE = {"threads": 128, "slot_bytes": 14336, "ctas_per_sm": 0}
 # Gate locations of the workloads' circuits (qubits x depth): one
 # single-qubit Pauli channel each in the noisy end-to-end leg.
 NOISE_LOCATIONS = {"cfg2-medium-40q-t12": 40 * 200, "cfg4-large-rank-85q-t20": 85 * 600}
@@ -440,7 +446,11 @@ def bench_batched(args, torch, dev, flush):
             "launch": "1 persistent kernel in a CUDA graph" if info["launches"] == 1
                       else f"{info['launches']} persistent kernels in a CUDA graph",
             "plain_launches": len(ws), "tuning": rec["tuning"], "work_items": info["items"],
-            "grid": info["grid"]}
+            "grid": info["grid"],
+            "issue_frac": NCU_THREAD_INST_PER_BATCH / (mb / 1e3) / issue_ceiling(torch, dev),
+            "issue_note": "ncu thread instructions of one batch at the launch shape "
+                          f"{NCU_BATCH_SHAPE} (this run: {rec['tuning']}) over the timed batch and "
+                          "148 SMs x 4 x 32 lanes x 1965 MHz"}
 
 
 class _PinnedRing:
